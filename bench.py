@@ -1,0 +1,351 @@
+"""Benchmark: LULESH sedov Lagrange step, zone-cycles/s on B200.
+
+Workload (BASELINE metric "zone-cycles/s at -s 100 on 1 B200"): one domain of
+-s 100 (1,000,000 hex elements, 1,030,301 nodes), FP64, 11 regions, balance 1,
+cost 1.  A step is one cycle (TimeIncrement + LagrangeLeapFrog) over the
+whole mesh.  State (~0.57 GB) is far larger than the 126 MB L2, so no flush
+is needed between cycles.
+
+  value   zone-cycles/s over exactly K device-timed cycles (CUDA events on the
+          library's stream), graph-captured, no host sync inside
+  e2e     the same metric through the host-driven C-ABI call
+          (lulesh_host_cycle): per cycle the host copies the time state in
+          (H2D) and reads time/dt/status back (D2H) and waits, as the
+          reference's loop does (TimeIncrement + checkErrors on the host)
+
+With --gpus N (torchrun), every rank runs its own -s 100 replica ("replicas
+only": the single-domain step has no exchange with other GPUs); value is
+the total over ranks using the max time over ranks.
+
+--impl reference times the reference's own OpenMP CPU build
+(oracle/_ref/lulesh_omp, compiled from LULESH/omp_4.0) on this host's cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "cuda-ipc-benchmarks_b200")
+ORACLE = os.path.join(REPO, "oracle")
+for _p in (PKG, ORACLE):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+NX = 100
+ZONES = NX ** 3
+METRIC = "zone-cycles/s at -s 100 on 1 B200"
+UNIT = "zone-cycles/s"
+# Algorithmic bytes per zone-cycle of each phase (compulsory traffic at the
+# four dependency boundaries of the step, FP64): force 152, nodal update 128,
+# kinematics + monoQ gradient 176, monoQ region + EOS + volume + dt 204.
+ALG_BYTES = {"force": 152.0, "nodal": 128.0, "kinematics": 176.0, "eos": 204.0}
+ALG_BYTES_STEP = 660.0
+LAUNCHES_PER_CYCLE = 5  # time_increment, force, nodal, kinematics, eos
+
+
+def measured_peak_gbs():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int, period_ms: int = 100):
+        self.gpu = gpu_index
+        self.period = period_ms
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        out_dir = os.path.join(REPO, "gpurun_out")
+        os.makedirs(out_dir, exist_ok=True)
+        self.path = os.path.join(out_dir, f"clocks_gpu{self.gpu}_{os.getpid()}.csv")
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", str(self.period)],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                t = [x.strip() for x in line.split(",")]
+                if len(t) < 9:
+                    continue
+                try:
+                    sm.append(float(t[1]))
+                    smax.append(float(t[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, t[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def omp_run(args, threads):
+    import oracle
+
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close")
+    out = subprocess.run([oracle.REF_OMP, *args], env=env, capture_output=True, text=True,
+                         timeout=600)
+    if out.returncode != 0:
+        raise RuntimeError(f"lulesh_omp {' '.join(args)} failed: {out.stderr[-300:]}")
+    return oracle.parse_report(out.stdout)
+
+
+def omp_best_threads(cores):
+    """The omp build needs >= 2 threads (1 segfaults at lulesh.cc:585) and
+    degrades badly when over-subscribed, so pick the best of a short sweep."""
+    cand = sorted({t for t in (2, 4, 8, 16, 32, 48, 64, 96, 128, 192, 256) if t <= cores}
+                  | ({cores} if cores >= 2 else set()))
+    best, best_rate = 2, 0.0
+    for t in cand:
+        r = omp_run(["-s", "40", "-i", "4"], t)
+        rate = 1e6 / r["grind"] if r.get("grind") else 0.0
+        if rate > best_rate:
+            best, best_rate = t, rate
+    return best, best_rate
+
+
+def cpu_baseline_sample(target_s=12.0):
+    """Reference omp_4.0 build on this host, bounded sample of -s 100."""
+    import oracle
+
+    if not os.path.exists(oracle.REF_OMP):
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                "sample": "oracle/_ref/lulesh_omp missing (built from the reference tree)"}
+    cores = host_cores()
+    threads, rate = omp_best_threads(cores)
+    its = int(max(2, min(40, target_s * rate / ZONES))) if rate > 0 else 3
+    r = omp_run(["-s", str(NX), "-i", str(its)], threads)
+    value = 1e6 / r["grind"]
+    return {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"lulesh_omp -s {NX} -i {its} (reference LULESH/omp_4.0, "
+                      f"OMP_NUM_THREADS={threads} of {cores} host cores, best of a "
+                      f"-s 40 thread sweep), elapsed {r['elapsed']:.2f} s"}
+
+
+def max_over_ranks(x: float, dist=None, device="cpu") -> float:
+    """Max of a per-rank timing over all ranks (any torch.distributed backend)."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(units_per_rank: int, seconds_max: float, world: int) -> float:
+    """Whole-job throughput: all ranks' units over the slowest rank's time."""
+    return world * units_per_rank / seconds_max
+
+
+def traffic_per_launch(kernel):
+    p = os.path.join(REPO, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return d["kernels"][kernel]["dram_bytes_per_launch_scaled"]
+    except Exception:
+        return None
+
+
+def run_ours(a, rank, world, local_rank):
+    import torch
+    import lulesh_b200 as L
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(local_rank)
+    dev = torch.cuda.current_device()
+    # a real (non-legacy) stream: the library captures its cycle graph on it
+    # and the timing events below are recorded on the same stream
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    total = a.warmup + a.steps
+    s = L.LuleshSet(nx=NX, its=-1, device=dev)
+    s.set_stream(stream.cuda_stream)
+    s.step(a.warmup)
+    s.sync()
+    st0 = s.state()
+    if st0["done"]:
+        raise RuntimeError("problem finished during warm-up")
+
+    clocks = ClockSampler(dev)
+    clocks.start()
+    time.sleep(0.3)  # let the sampler start before the timed region
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    s.step(a.steps)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ck = clocks.stop()
+    ms = t0.elapsed_time(t1)
+    st = s.state()
+    if st["status"] != 0 or st["cycle"] != total or st["done"]:
+        raise RuntimeError(f"run did not complete {total} cycles cleanly: {st}")
+    ms = max_over_ranks(ms, dist, "cuda")
+    value = aggregate_rate(ZONES * a.steps, ms / 1e3, world)
+
+    # per-phase device times (events around each phase, same stream)
+    phases = s.profile_phases(a.profile_cycles)
+    dom = max((k for k in ALG_BYTES), key=lambda k: phases.get(k, 0.0))
+    peak, peak_kind = measured_peak_gbs()
+    ach = ALG_BYTES[dom] * ZONES / (phases[dom] / 1e3) / 1e9
+    step_ms_sum = sum(phases.values())
+    ach_step = ALG_BYTES_STEP * ZONES / (ms / a.steps / 1e3) / 1e9
+
+    # end-to-end through the host-driven C-ABI call
+    e2e_n = min(a.steps, a.e2e_cycles)
+    _, cur = s.host_cycle(None)
+    if dist:
+        dist.barrier()
+    tw = time.perf_counter()
+    for _ in range(e2e_n):
+        stc, cur = s.host_cycle(cur)
+        if stc != 0:
+            raise RuntimeError(f"host cycle failed: {stc}")
+    e2e_s = max_over_ranks(time.perf_counter() - tw, dist, "cuda")
+    e2e_val = aggregate_rate(ZONES * e2e_n, e2e_s, world)
+    energy = s.origin_energy()
+    s.close()
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    cpu = cpu_baseline_sample() if world == 1 else None
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: sedov blast generated in code (reference problem setup)",
+        "config": {"workload": "LULESH sedov single domain -s 100 (1,000,000 elements), "
+                               "FP64, -r 11 -b 1 -c 1, one cycle per step",
+                   "nx": NX, "zones": ZONES, "regions": 11, "balance": 1, "cost": 1,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "state ~0.57 GB > 126 MB L2: no flush needed"},
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 16,
+                "d2h_bytes_per_step": 80, "cycles": e2e_n,
+                "how": "lulesh_host_cycle: H2D time/dt, one graph-launched cycle, "
+                       "D2H time-control record, host waits each cycle"},
+        "gpu_launches": LAUNCHES_PER_CYCLE * a.steps,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak,
+                     "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind,
+                     "alg_bytes_per_zone": ALG_BYTES[dom],
+                     "traffic": traffic_per_launch(dom)},
+        "roofline_step": {"achieved": ach_step, "frac": ach_step / peak,
+                          "alg_bytes_per_zone_cycle": ALG_BYTES_STEP},
+        "phases_ms": phases, "phases_sum_ms": step_ms_sum,
+        "clocks": ck, "origin_energy": energy, "cycles_run": total,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_reference(a, rank, world):
+    if rank != 0:
+        return
+    import oracle
+
+    if not os.path.exists(oracle.REF_OMP):
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/lulesh_omp was not built"}))
+        return
+    cores = host_cores()
+    threads, rate = omp_best_threads(cores)
+    # warm-up run, then K cycles of the reference's own timed loop
+    omp_run(["-s", str(NX), "-i", str(max(1, min(a.warmup, 3)))], threads)
+    r = omp_run(["-s", str(NX), "-i", str(a.steps)], threads)
+    value = 1e6 / r["grind"]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": r["elapsed"] * 1e3 / a.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: sedov blast generated in code",
+        "config": {"workload": "LULESH sedov single domain -s 100 (1,000,000 elements), "
+                               "FP64, -r 11 -b 1 -c 1, one cycle per step", "nx": NX},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"lulesh_omp -s {NX} -i {a.steps} (LULESH/omp_4.0), "
+                                   f"OMP_NUM_THREADS={threads} of {cores}"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "origin_energy": r.get("energy"),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--profile-cycles", dest="profile_cycles", type=int, default=5)
+    ap.add_argument("--e2e-cycles", dest="e2e_cycles", type=int, default=100)
+    a = ap.parse_args()
+    if a.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if a.warmup + a.steps > 3000:
+        ap.error("-s 100 reaches t = 0.01 after ~3500 cycles: keep warmup + steps <= 3000")
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(a.gpus)))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        run_reference(a, rank, world)
+    else:
+        run_ours(a, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,63 @@
+// host_probe.cpp -- host-only entry points into the domain setup, built as
+// liblulesh_host.so (no CUDA) so the CPU test suite can check the setup
+// arithmetic and index layout against the oracle without a GPU.  Not part
+// of the drop-in ABI (include/lulesh_b200.h).
+#include <cstring>
+
+#include "host_setup.hpp"
+
+extern "C" {
+
+// The first n values of rand() after srand(seed).
+void lulesh_host_rand(unsigned seed, int n, int *out)
+{
+    lulesh::GlibcRand r(seed);
+    for (int i = 0; i < n; ++i) out[i] = r.next();
+}
+
+// Build one domain and copy the named array into out (capacity `cap`
+// elements of the array's type); returns the array length, -1 if unknown.
+long lulesh_host_domain_field(int nx, int tp, int col, int row, int plane, int rank,
+                              int numReg, int balance, int cost, int global_mass,
+                              const char *name, void *out, long cap)
+{
+    lulesh::HostDomain d;
+    lulesh::build_domain(d, nx, tp, col, row, plane, rank, numReg, balance, cost,
+                         global_mass != 0);
+    struct I {
+        const char *n;
+        const std::vector<int> *v;
+    } ints[] = {{"nodelist", &d.nodelist}, {"lxim", &d.lxim}, {"lxip", &d.lxip},
+                {"letam", &d.letam}, {"letap", &d.letap}, {"lzetam", &d.lzetam},
+                {"lzetap", &d.lzetap}, {"elemBC", &d.elemBC},
+                {"nodeElemCount", &d.nodeElemCount}, {"nodeElemStart", &d.nodeElemStart},
+                {"nodeElemCornerList", &d.nodeElemCornerList}, {"symmX", &d.symmX},
+                {"symmY", &d.symmY}, {"symmZ", &d.symmZ}, {"matElemlist", &d.matElemlist},
+                {"regElemSize", &d.regElemSize}, {"regCSR", &d.regCSR},
+                {"regReps", &d.regReps}, {"regNumList", &d.regNumList},
+                {"regElemlist", &d.regElemlist}, {"regSorted", &d.regSorted}};
+    struct R {
+        const char *n;
+        const std::vector<double> *v;
+    } reals[] = {{"x", &d.x}, {"y", &d.y}, {"z", &d.z}, {"volo", &d.volo},
+                 {"elemMass", &d.elemMass}, {"nodalMass", &d.nodalMass}, {"e", &d.e}};
+    for (const I &i : ints)
+        if (!std::strcmp(i.n, name)) {
+            long n = (long)i.v->size();
+            if (out && cap >= n) std::memcpy(out, i.v->data(), sizeof(int) * n);
+            return n;
+        }
+    for (const R &r : reals)
+        if (!std::strcmp(r.n, name)) {
+            long n = (long)r.v->size();
+            if (out && cap >= n) std::memcpy(out, r.v->data(), sizeof(double) * n);
+            return n;
+        }
+    if (!std::strcmp(name, "deltatime")) {
+        if (out && cap >= 1) *(double *)out = d.deltatime;
+        return 1;
+    }
+    return -1;
+}
+
+}  // extern "C"

@@ -1,0 +1,59 @@
+// host_setup.hpp -- host-side construction of LULESH domains.
+//
+// Builds, on the host, every array NewDomain (LULESH/cuda/src/lulesh.cu:
+// 750-1221) builds for the structured (-s) mesh, in the same order and with
+// the same arithmetic, so the device arena can be filled with one copy per
+// array.  Compiled without FMA contraction, like the reference's host code.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "lulesh_dev.h"
+
+namespace lulesh {
+
+// glibc's rand()/srand() (TYPE_3 additive feedback generator, 31 words of
+// state), restated so region sets match the reference's srand(rank)/rand()
+// without touching the process-wide libc state.
+class GlibcRand {
+  public:
+    explicit GlibcRand(unsigned seed);
+    int next();  // same sequence as rand() after srand(seed)
+
+  private:
+    int32_t r_[34];
+    int idx_;
+};
+
+struct HostDomain {
+    int nx = 0, en = 0, numElem = 0, numNode = 0, Ep = 0, allElem = 0;
+    int tp = 1, col = 0, row = 0, plane = 0, rank = 0;
+    int rowMin = 0, rowMax = 0, colMin = 0, colMax = 0, planeMin = 0, planeMax = 0;
+    int numReg = 0, balance = 1, cost = 1;
+    int numSymmX = 0, numSymmY = 0, numSymmZ = 0;
+    int ghost[6] = {-1, -1, -1, -1, -1, -1};
+    std::vector<int> nodelist, lxim, lxip, letam, letap, lzetam, lzetap, elemBC;
+    std::vector<int> nodeElemCount, nodeElemStart, nodeElemCornerList;
+    std::vector<int> symmX, symmY, symmZ, matElemlist;
+    std::vector<int> regElemSize, regCSR, regReps, regNumList, regElemlist, regSorted;
+    std::vector<double> x, y, z, volo, elemMass, nodalMass, e;
+    double einit = 0.0;
+    double deltatime = 0.0;  // initial dt of this domain, lulesh.cu:1205
+};
+
+// Reference parameter block, lulesh.cu:1125-1158.
+Params default_params();
+
+// Build one domain of a tp^3 decomposition at (col,row,plane).
+// `global_mass` computes nodalMass as the single-domain sum over the
+// problem's elements in ascending global index (what the reference's
+// single-rank run produces); otherwise only this domain's elements
+// contribute (what each rank holds before the init-time CommSBN).
+void build_domain(HostDomain &d, int nx, int tp, int col, int row, int plane,
+                  int rank, int numReg, int balance, int cost, bool global_mass);
+
+// CalcElemVolume (lulesh.cu:221-307), host copy used at setup.
+double elem_volume_host(const double *x, const double *y, const double *z);
+
+}  // namespace lulesh

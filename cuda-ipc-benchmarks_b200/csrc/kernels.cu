@@ -1,0 +1,789 @@
+// kernels.cu -- the per-cycle kernels of the LULESH Lagrange leapfrog step.
+//
+// One cycle is five launches (captured in one CUDA graph):
+//   time_increment  TimeIncrement on the device (lulesh.cu:1400-1461)
+//   force           CalcVolumeForceForElems_kernel (lulesh.cu:2080-2259):
+//                   stress + FB hourglass corner forces per element
+//   nodal           AddNodeForcesFromElems + CalcAccelerationForNodes +
+//                   ApplyAccelerationBoundaryConditionsForNodes +
+//                   CalcPositionAndVelocityForNodes (lulesh.cu:1715-1751,
+//                   2925-3044) fused: corners summed in corner order with
+//                   no atomics, then the node update
+//   kinematics      CalcKinematicsAndMonotonicQGradient_kernel
+//                   (lulesh.cu:3343-3507)
+//   eos             CalcMonotonicQRegionForElems_kernel +
+//                   ApplyMaterialPropertiesAndUpdateVolume_kernel +
+//                   CalcTimeConstraintsForElems (lulesh.cu:3554-3725,
+//                   3988-4097, 4216-4403) fused; the dt minimum is reduced
+//                   with warp shuffles and one 64-bit atomicMin per block
+// Subdomain sets add two halo kernels (PosVel sync, MonoQ ghosts).
+#include <climits>
+#include <cstdint>
+
+#include "elem_math.cuh"
+#include "kernels.cuh"
+
+namespace lulesh {
+
+// ---------------------------------------------------------------------------
+// time increment
+
+__device__ __forceinline__ unsigned long long dbits(double v)
+{
+    return (unsigned long long)__double_as_longlong(v);
+}
+
+__global__ void k_time_increment(TimeCtl *tcs, int ntc, Params P)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ntc) return;
+    TimeCtl &T = tcs[i];
+    T.active = 0;
+    if (T.done) return;
+    // checkErrors (lulesh.cu:2879-2892): a cycle that raised an error ends
+    // the job before the next one starts
+    if (T.bad_vol != INT_MAX) {
+        T.status = -1;
+        T.done = 1;
+        return;
+    }
+    if (T.bad_q != INT_MAX) {
+        T.status = -2;
+        T.done = 1;
+        return;
+    }
+    // while (time < stoptime) ... if (its == num_iters) break (lulesh.cu:4858-4873)
+    if (!(T.time < P.stoptime) || (T.its_cap > 0 && T.cycle >= T.its_cap)) {
+        T.done = 1;
+        return;
+    }
+    if (T.cycle != 0) {
+        // the previous cycle's CalcTimeConstraintsForElems result
+        T.dtcourant = __longlong_as_double((long long)T.min_courant);
+        T.dthydro = __longlong_as_double((long long)T.min_hydro);
+    }
+    T.min_courant = dbits(1.0e+20);
+    T.min_hydro = dbits(1.0e+20);
+
+    double targetdt = P.stoptime - T.time;
+    if ((P.dtfixed <= 0.0) && (T.cycle != 0)) {
+        double ratio;
+        double gnewdt = 1.0e+20;
+        double newdt;
+        if (T.dtcourant < gnewdt) gnewdt = T.dtcourant / 2.0;
+        if (T.dthydro < gnewdt) gnewdt = T.dthydro * 2.0 / 3.0;
+        newdt = gnewdt;
+        const double olddt = T.deltatime;
+        ratio = newdt / olddt;
+        if (ratio >= 1.0) {
+            if (ratio < P.deltatimemultlb)
+                newdt = olddt;
+            else if (ratio > P.deltatimemultub)
+                newdt = olddt * P.deltatimemultub;
+        }
+        if (newdt > P.dtmax) newdt = P.dtmax;
+        T.deltatime = newdt;
+    }
+    // try to prevent very small scaling on the next cycle
+    if ((targetdt > T.deltatime) && (targetdt < (4.0 * T.deltatime / 3.0)))
+        targetdt = 2.0 * T.deltatime / 3.0;
+    if (targetdt < T.deltatime) T.deltatime = targetdt;
+    T.time += T.deltatime;
+    ++T.cycle;
+    T.active = 1;
+}
+
+void launch_time_increment(TimeCtl *tcs, int ntc, Params P, cudaStream_t s)
+{
+    const int b = 128;
+    k_time_increment<<<(ntc + b - 1) / b, b, 0, s>>>(tcs, ntc, P);
+}
+
+// ---------------------------------------------------------------------------
+// structured-mesh indexing helpers
+
+// corner j of an element sits at lattice offset (CX[j], CY[j], CZ[j]) from
+// the element's corner 0 (nodelist order of BuildMesh, lulesh.cu:730-737)
+__device__ __constant__ int kCX[8] = {0, 1, 1, 0, 0, 1, 1, 0};
+__device__ __constant__ int kCY[8] = {0, 0, 1, 1, 0, 0, 1, 1};
+__device__ __constant__ int kCZ[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+
+__device__ __forceinline__ void elem_nodes(const DomDev &D, int el, int n[8])
+{
+    const int nx = D.nx, en = D.en;
+    const int ix = el % nx;
+    const int t = el / nx;
+    const int iy = t % nx;
+    const int iz = t / nx;
+    const int n0 = (iz * en + iy) * en + ix;
+    n[0] = n0;
+    n[1] = n0 + 1;
+    n[2] = n0 + en + 1;
+    n[3] = n0 + en;
+    n[4] = n0 + en * en;
+    n[5] = n0 + en * en + 1;
+    n[6] = n0 + en * en + en + 1;
+    n[7] = n0 + en * en + en;
+}
+
+// ---------------------------------------------------------------------------
+// force: CalcVolumeForceForElems_kernel, lulesh.cu:2080-2259
+
+template <bool HG>
+__global__ void __launch_bounds__(kElemBlock) k_force(SetArgs a, Params P)
+{
+    const int2 blk = a.blocks[blockIdx.x];
+    const DomDev &D = a.doms[blk.x];
+    TimeCtl &T = a.tcs[D.tc];
+    if (!T.active) return;
+    const int elem = blk.y + threadIdx.x;
+    if (elem >= D.numElem) return;
+
+    double xn[8], yn[8], zn[8];
+    double dvdxn[8], dvdyn[8], dvdzn[8];
+    double hgfx[8], hgfy[8], hgfz[8];
+    double hourgam[8][4];
+    double coefficient;
+
+    double volume = D.v[elem];
+    double det = D.volo[elem] * volume;
+    if (volume < 0.) atomicMin(&T.bad_vol, elem);
+    const double ss1 = D.ss[elem];
+    const double mass1 = D.elemMass[elem];
+    const double sigxx = -D.p[elem] - D.q[elem];
+
+    int n[8];
+    elem_nodes(D, elem, n);
+    const double volinv = 1.0 / det;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) xn[i] = D.x[n[i]];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) yn[i] = D.y[n[i]];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) zn[i] = D.z[n[i]];
+
+    const double hourg = P.hgcoef;
+    const double volume13 = cbrt(det);
+    coefficient = -hourg * 0.01 * ss1 * mass1 / volume13;
+
+    elem_volume_derivative(dvdxn, dvdyn, dvdzn, xn, yn, zn);
+    hourglass_modes(xn, yn, zn, dvdxn, dvdyn, dvdzn, hourgam, volinv);
+
+    double B[3][8];
+    shape_function_derivatives(xn, yn, zn, B, &det);
+    elem_node_normals(B[0], B[1], B[2], xn, yn, zn);
+    if (det < 0.) atomicMin(&T.bad_vol, elem);
+
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        hgfx[i] = -(sigxx * B[0][i]);
+        hgfy[i] = -(sigxx * B[1][i]);
+        hgfz[i] = -(sigxx * B[2][i]);
+    }
+    if (HG) {
+        double vel[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) vel[i] = D.xd[n[i]];
+        fb_hourglass_component(vel, hourgam, coefficient, hgfx);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) vel[i] = D.yd[n[i]];
+        fb_hourglass_component(vel, hourgam, coefficient, hgfy);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) vel[i] = D.zd[n[i]];
+        fb_hourglass_component(vel, hourgam, coefficient, hgfz);
+    }
+    const int Ep = D.Ep;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        D.fx_elem[elem + Ep * k] = hgfx[k];
+        D.fy_elem[elem + Ep * k] = hgfy[k];
+        D.fz_elem[elem + Ep * k] = hgfz[k];
+    }
+}
+
+void launch_force(const SetArgs &a, int nblocks, Params P, cudaStream_t s)
+{
+    if (P.hgcoef > 0.0)
+        k_force<true><<<nblocks, kElemBlock, 0, s>>>(a, P);
+    else
+        k_force<false><<<nblocks, kElemBlock, 0, s>>>(a, P);
+}
+
+// ---------------------------------------------------------------------------
+// nodal: corner gather (in nodeElemCornerList order) + node update
+
+// Sum the corner forces around node (px,py,pz) of domain D in corner order
+// j = 0..7, the order nodeElemCornerList has on a structured mesh
+// (lulesh.cu:1082-1091).  A corner whose element lies in a neighbouring
+// subdomain is read from that subdomain's corner array: the result equals
+// the undecomposed mesh's sum bit for bit.
+__device__ __forceinline__ void gather_corners(const DomDev *doms, const DomDev &D, int px,
+                                               int py, int pz, double &fx, double &fy,
+                                               double &fz)
+{
+    const int nx = D.nx;
+    fx = fy = fz = 0.0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int ex = px - kCX[j], ey = py - kCY[j], ez = pz - kCZ[j];
+        const bool inside = (unsigned)ex < (unsigned)nx && (unsigned)ey < (unsigned)nx &&
+                            (unsigned)ez < (unsigned)nx;
+        if (inside) {
+            const int idx = j * D.Ep + (ez * nx + ey) * nx + ex;
+            fx += D.fx_elem[idx];
+            fy += D.fy_elem[idx];
+            fz += D.fz_elem[idx];
+        } else if (D.tp > 1) {
+            const int sx = (ex < 0) ? -1 : (ex >= nx ? 1 : 0);
+            const int sy = (ey < 0) ? -1 : (ey >= nx ? 1 : 0);
+            const int sz = (ez < 0) ? -1 : (ez >= nx ? 1 : 0);
+            const int nb = D.nbr[(sx + 1) + 3 * (sy + 1) + 9 * (sz + 1)];
+            if (nb >= 0) {
+                const DomDev &N = doms[nb];
+                const int lx = ex - sx * nx, ly = ey - sy * nx, lz = ez - sz * nx;
+                const int idx = j * N.Ep + (lz * nx + ly) * nx + lx;
+                fx += N.fx_elem[idx];
+                fy += N.fy_elem[idx];
+                fz += N.fz_elem[idx];
+            }
+        }
+    }
+}
+
+// MODE 0: gather every corner (neighbour subdomains included) and update
+//         the node: the fused form of the SBN exchange + node update.
+// MODE 1: AddNodeForcesFromElems over this domain's own corners only,
+//         writing fx/fy/fz (the partial sums the reference exchanges).
+// MODE 2: the node update from fx/fy/fz (after CommSBN added neighbours).
+template <int MODE>
+__global__ void __launch_bounds__(kNodeBlock) k_nodal(SetArgs a, Params P)
+{
+    const int2 blk = a.blocks[blockIdx.x];
+    const DomDev &D = a.doms[blk.x];
+    const TimeCtl &T = a.tcs[D.tc];
+    if (!T.active) return;
+    const int i = blk.y + threadIdx.x;
+    if (i >= D.numNode) return;
+    const int en = D.en;
+    const int px = i % en;
+    const int t = i / en;
+    const int py = t % en;
+    const int pz = t / en;
+
+    double fx, fy, fz;
+    if (MODE == 0) {
+        gather_corners(a.doms, D, px, py, pz, fx, fy, fz);
+    } else if (MODE == 1) {
+        DomDev L = D;
+        L.tp = 1;  // own corners only
+        gather_corners(a.doms, L, px, py, pz, fx, fy, fz);
+        D.fx[i] = fx;
+        D.fy[i] = fy;
+        D.fz[i] = fz;
+        return;
+    } else {
+        fx = D.fx[i];
+        fy = D.fy[i];
+        fz = D.fz[i];
+    }
+
+    // CalcAccelerationForNodes_kernel, lulesh.cu:2926-2939
+    const double one_over_nMass = 1. / D.nodalMass[i];
+    double xdd = fx * one_over_nMass;
+    double ydd = fy * one_over_nMass;
+    double zdd = fz * one_over_nMass;
+    // ApplyAccelerationBoundaryConditionsForNodes: symmetry planes are the
+    // px/py/pz == 0 node sets of the domains at the mesh origin faces
+    if (D.col == 0 && px == 0) xdd = 0.0;
+    if (D.row == 0 && py == 0) ydd = 0.0;
+    if (D.plane == 0 && pz == 0) zdd = 0.0;
+
+    // CalcPositionAndVelocityForNodes_kernel, lulesh.cu:2999-3028
+    const double dt = T.deltatime;
+    const double u_cut = P.u_cut;
+    double xdtmp = D.xd[i] + xdd * dt;
+    double ydtmp = D.yd[i] + ydd * dt;
+    double zdtmp = D.zd[i] + zdd * dt;
+    if (fabs(xdtmp) < u_cut) xdtmp = 0.0;
+    if (fabs(ydtmp) < u_cut) ydtmp = 0.0;
+    if (fabs(zdtmp) < u_cut) zdtmp = 0.0;
+    D.x[i] += xdtmp * dt;
+    D.y[i] += ydtmp * dt;
+    D.z[i] += zdtmp * dt;
+    D.xd[i] = xdtmp;
+    D.yd[i] = ydtmp;
+    D.zd[i] = zdtmp;
+    if (a.materialize) {
+        if (MODE == 0) {
+            D.fx[i] = fx;
+            D.fy[i] = fy;
+            D.fz[i] = fz;
+        }
+        D.xdd[i] = xdd;
+        D.ydd[i] = ydd;
+        D.zdd[i] = zdd;
+    }
+}
+
+void launch_nodal(const SetArgs &a, int nblocks, Params P, cudaStream_t s)
+{
+    k_nodal<0><<<nblocks, kNodeBlock, 0, s>>>(a, P);
+}
+
+void launch_nodal_gather_local(const SetArgs &a, int nblocks, cudaStream_t s)
+{
+    k_nodal<1><<<nblocks, kNodeBlock, 0, s>>>(a, Params{});
+}
+
+void launch_nodal_update(const SetArgs &a, int nblocks, Params P, cudaStream_t s)
+{
+    k_nodal<2><<<nblocks, kNodeBlock, 0, s>>>(a, P);
+}
+
+// ---------------------------------------------------------------------------
+// kinematics: CalcKinematicsAndMonotonicQGradient_kernel, lulesh.cu:3343-3507
+
+__global__ void __launch_bounds__(kElemBlock) k_kinematics(SetArgs a, Params P)
+{
+    const int2 blk = a.blocks[blockIdx.x];
+    const DomDev &D = a.doms[blk.x];
+    TimeCtl &T = a.tcs[D.tc];
+    if (!T.active) return;
+    const int k = blk.y + threadIdx.x;
+    if (k >= D.numElem) return;
+
+    double B[3][8];
+    double x_local[8], y_local[8], z_local[8];
+    double xd_local[8], yd_local[8], zd_local[8];
+    double Dv[3];
+    int nodes[8];
+    elem_nodes(D, k, nodes);
+#pragma unroll
+    for (int l = 0; l < 8; ++l) x_local[l] = D.x[nodes[l]];
+#pragma unroll
+    for (int l = 0; l < 8; ++l) y_local[l] = D.y[nodes[l]];
+#pragma unroll
+    for (int l = 0; l < 8; ++l) z_local[l] = D.z[nodes[l]];
+
+    const double volume = elem_volume(x_local, y_local, z_local);
+    const double relativeVolume = volume / D.volo[k];
+    D.vnew[k] = relativeVolume;
+    D.delv[k] = relativeVolume - D.v[k];
+    D.arealg[k] = elem_characteristic_length(x_local, y_local, z_local, volume);
+
+#pragma unroll
+    for (int l = 0; l < 8; ++l) {
+        const int g = nodes[l];
+        xd_local[l] = D.xd[g];
+        yd_local[l] = D.yd[g];
+        zd_local[l] = D.zd[g];
+    }
+    const double dt2 = 0.5 * T.deltatime;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        x_local[j] -= dt2 * xd_local[j];
+        y_local[j] -= dt2 * yd_local[j];
+        z_local[j] -= dt2 * zd_local[j];
+    }
+    double detJ;
+    shape_function_derivatives(x_local, y_local, z_local, B, &detJ);
+    elem_velocity_divergence(xd_local, yd_local, zd_local, B, detJ, Dv);
+    const double vdovNew = Dv[0] + Dv[1] + Dv[2];
+    D.vdov[k] = vdovNew;
+
+    const double vol = D.volo[k] * relativeVolume;
+    // undo the half-step shift exactly as the reference does (the restored
+    // coordinates can differ from the originals in the last bit)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        x_local[j] += dt2 * xd_local[j];
+        y_local[j] += dt2 * yd_local[j];
+        z_local[j] += dt2 * zd_local[j];
+    }
+    double dxz, dvz, dxx, dvx, dxe, dve;
+    mono_gradient(x_local, y_local, z_local, xd_local, yd_local, zd_local, vol, &dxz, &dvz,
+                  &dxx, &dvx, &dxe, &dve);
+    D.delx_zeta[k] = dxz;
+    D.delv_zeta[k] = dvz;
+    D.delx_xi[k] = dxx;
+    D.delv_xi[k] = dvx;
+    D.delx_eta[k] = dxe;
+    D.delv_eta[k] = dve;
+    if (relativeVolume < 0) atomicMin(&T.bad_vol, k);
+}
+
+void launch_kinematics(const SetArgs &a, int nblocks, Params P, cudaStream_t s)
+{
+    k_kinematics<<<nblocks, kElemBlock, 0, s>>>(a, P);
+}
+
+// ---------------------------------------------------------------------------
+// eos: monotonic Q region + EOS + volume update + dt constraints
+
+// one direction of the monotonic limiter, lulesh.cu:3595-3624
+__device__ __forceinline__ double mono_limiter(const double *delv, int i, int bc, int mmask,
+                                               int msymm, int mfree, int pmask, int psymm,
+                                               int pfree, int lm, int lp, double mult,
+                                               double maxslope, double ptiny)
+{
+    const double norm = 1. / (delv[i] + ptiny);
+    double delvm, delvp;
+    const int mb = bc & mmask, pb = bc & pmask;
+    if (mb == msymm)
+        delvm = delv[i];
+    else if (mb == mfree)
+        delvm = 0.0;
+    else
+        delvm = delv[lm];  // 0 or *_COMM: neighbour or ghost element
+    if (pb == psymm)
+        delvp = delv[i];
+    else if (pb == pfree)
+        delvp = 0.0;
+    else
+        delvp = delv[lp];
+    delvm = delvm * norm;
+    delvp = delvp * norm;
+    double phi = .5 * (delvm + delvp);
+    delvm *= mult;
+    delvp *= mult;
+    if (delvm < phi) phi = delvm;
+    if (delvp < phi) phi = delvp;
+    if (phi < 0.) phi = 0.;
+    if (phi > maxslope) phi = maxslope;
+    return phi;
+}
+
+// CalcPressureForElems_device, lulesh.cu:3764-3791
+__device__ __forceinline__ void calc_pressure(double &p_new, double &bvc, double &pbvc,
+                                              double &e_old, double &compression,
+                                              double &vnewc, double pmin, double p_cut,
+                                              double eosvmax)
+{
+    const double c1s = 2.0 / 3.0;
+    double p_temp;
+    bvc = c1s * (compression + 1.);
+    pbvc = c1s;
+    p_temp = bvc * e_old;
+    if (fabs(p_temp) < p_cut) p_temp = 0.0;
+    if (vnewc >= eosvmax) p_temp = 0.0;
+    if (p_temp < pmin) p_temp = pmin;
+    p_new = p_temp;
+}
+
+// CalcEnergyForElems_device, lulesh.cu:3867-3974
+__device__ __forceinline__ void calc_energy(double &p_new, double &e_new, double &q_new,
+                                            double &bvc, double &pbvc, double &p_old,
+                                            double &e_old, double &q_old, double &compression,
+                                            double &compHalfStep, double &vnewc, double &work,
+                                            double &delvc, double pmin, double p_cut,
+                                            double e_cut, double q_cut, double emin,
+                                            double &qq, double &ql, double &rho0,
+                                            double &eosvmax)
+{
+    const double sixth = 1.0 / 6.0;
+    double pHalfStep;
+    e_new = e_old - 0.5 * delvc * (p_old + q_old) + 0.5 * work;
+    if (e_new < emin) e_new = emin;
+    calc_pressure(pHalfStep, bvc, pbvc, e_new, compHalfStep, vnewc, pmin, p_cut, eosvmax);
+    const double vhalf = 1. / (1. + compHalfStep);
+    if (delvc > 0.) {
+        q_new = 0.;
+    } else {
+        double ssc = (pbvc * e_new + vhalf * vhalf * bvc * pHalfStep) / rho0;
+        if (ssc <= .1111111e-36)
+            ssc = .3333333e-18;
+        else
+            ssc = sqrt(ssc);
+        q_new = (ssc * ql + qq);
+    }
+    e_new = e_new + 0.5 * delvc * (3.0 * (p_old + q_old) - 4.0 * (pHalfStep + q_new));
+    e_new += 0.5 * work;
+    if (fabs(e_new) < e_cut) e_new = 0.;
+    if (e_new < emin) e_new = emin;
+    calc_pressure(p_new, bvc, pbvc, e_new, compression, vnewc, pmin, p_cut, eosvmax);
+    double q_tilde;
+    if (delvc > 0.) {
+        q_tilde = 0.;
+    } else {
+        double ssc = (pbvc * e_new + vnewc * vnewc * bvc * p_new) / rho0;
+        if (ssc <= .1111111e-36)
+            ssc = .3333333e-18;
+        else
+            ssc = sqrt(ssc);
+        q_tilde = (ssc * ql + qq);
+    }
+    e_new = e_new - (7.0 * (p_old + q_old) - 8.0 * (pHalfStep + q_new) + (p_new + q_tilde)) *
+                        delvc * sixth;
+    if (fabs(e_new) < e_cut) e_new = 0.;
+    if (e_new < emin) e_new = emin;
+    calc_pressure(p_new, bvc, pbvc, e_new, compression, vnewc, pmin, p_cut, eosvmax);
+    if (delvc <= 0.) {
+        double ssc = (pbvc * e_new + vnewc * vnewc * bvc * p_new) / rho0;
+        if (ssc <= .1111111e-36)
+            ssc = .3333333e-18;
+        else
+            ssc = sqrt(ssc);
+        q_new = (ssc * ql + qq);
+        if (fabs(q_new) < q_cut) q_new = 0.;
+    }
+}
+
+__device__ __forceinline__ double warp_min(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__global__ void __launch_bounds__(kElemBlock) k_eos(SetArgs a, Params P)
+{
+    const int2 blk = a.blocks[blockIdx.x];
+    const DomDev &D = a.doms[blk.x];
+    TimeCtl &T = a.tcs[D.tc];
+    if (!T.active) return;  // uniform per block
+    const int i = blk.y + threadIdx.x;
+    double dtc = 1.0e+20, dth = 1.0e+20;
+    if (i < D.numElem) {
+        const int zidx = D.regElemlist[i];
+
+        // ---- CalcMonotonicQRegionForElems_kernel, lulesh.cu:3586-3724
+        const double ptiny = 1.e-36;
+        const int bcMask = D.elemBC[zidx];
+        const double mult = P.monoq_limiter_mult, maxs = P.monoq_max_slope;
+        const double phixi =
+            mono_limiter(D.delv_xi, zidx, bcMask, XI_M, XI_M_SYMM, XI_M_FREE, XI_P, XI_P_SYMM,
+                         XI_P_FREE, D.lxim[zidx], D.lxip[zidx], mult, maxs, ptiny);
+        const double phieta =
+            mono_limiter(D.delv_eta, zidx, bcMask, ETA_M, ETA_M_SYMM, ETA_M_FREE, ETA_P,
+                         ETA_P_SYMM, ETA_P_FREE, D.letam[zidx], D.letap[zidx], mult, maxs, ptiny);
+        const double phizeta =
+            mono_limiter(D.delv_zeta, zidx, bcMask, ZETA_M, ZETA_M_SYMM, ZETA_M_FREE, ZETA_P,
+                         ZETA_P_SYMM, ZETA_P_FREE, D.lzetam[zidx], D.lzetap[zidx], mult, maxs,
+                         ptiny);
+        const double vdov_z = D.vdov[zidx];
+        const double vnew_z = D.vnew[zidx];
+        double qlin, qquad;
+        if (vdov_z > 0.) {
+            qlin = 0.;
+            qquad = 0.;
+        } else {
+            double delvxxi = D.delv_xi[zidx] * D.delx_xi[zidx];
+            double delvxeta = D.delv_eta[zidx] * D.delx_eta[zidx];
+            double delvxzeta = D.delv_zeta[zidx] * D.delx_zeta[zidx];
+            if (delvxxi > 0.) delvxxi = 0.;
+            if (delvxeta > 0.) delvxeta = 0.;
+            if (delvxzeta > 0.) delvxzeta = 0.;
+            const double rho = D.elemMass[zidx] / (D.volo[zidx] * vnew_z);
+            qlin = -P.qlc_monoq * rho *
+                   (delvxxi * (1. - phixi) + delvxeta * (1. - phieta) +
+                    delvxzeta * (1. - phizeta));
+            qquad = P.qqc_monoq * rho *
+                    (delvxxi * delvxxi * (1. - phixi * phixi) +
+                     delvxeta * delvxeta * (1. - phieta * phieta) +
+                     delvxzeta * delvxzeta * (1. - phizeta * phizeta));
+        }
+        const double q_old_z = D.q[zidx];
+        if (q_old_z > P.qstop) atomicMin(&T.bad_q, zidx);
+        if (a.materialize) {
+            D.qq[zidx] = qquad;
+            D.ql[zidx] = qlin;
+        }
+
+        // ---- ApplyMaterialPropertiesAndUpdateVolume_kernel, lulesh.cu:4025-4096
+        double eosvmin = P.eosvmin, eosvmax = P.eosvmax;
+        double vnewc = vnew_z;
+        if (eosvmin != 0.) {
+            if (vnewc < eosvmin) vnewc = eosvmin;
+        }
+        if (eosvmax != 0.) {
+            if (vnewc > eosvmax) vnewc = eosvmax;
+        }
+        double vc = D.v[zidx];
+        if (eosvmin != 0.) {
+            if (vc < eosvmin) vc = eosvmin;
+        }
+        if (eosvmax != 0.) {
+            if (vc > eosvmax) vc = eosvmax;
+        }
+        if (vc <= 0.) atomicMin(&T.bad_vol, zidx);
+
+        // giveMyRegion (lulesh.cu:3976-3984): regCSR holds region ends
+        int region = D.numReg - 1;
+        for (int r = 0; r < D.numReg - 1; ++r)
+            if (i < D.regCSR[r]) {
+                region = r;
+                break;
+            }
+        const int rep = D.regReps[region];
+
+        double e_old, delvc, p_old, q_old, compression, compHalfStep, qq_old, ql_old, work;
+        double p_new = 0., e_new = 0., q_new = 0., bvc = 0., pbvc = 0.;
+        const double e_temp = D.e[zidx];
+        const double p_temp = D.p[zidx];
+        const double q_temp = q_old_z;
+        const double qq_temp = qquad;
+        const double ql_temp = qlin;
+        const double delvc_temp = D.delv[zidx];
+        double rho0 = P.refdens;
+        // The reference's cost model: every rep re-evaluates the EOS from
+        // the same inputs (the loop is pure), lulesh.cu:4045-4083.
+        for (int r = 0; r < rep; r++) {
+            e_old = e_temp;
+            p_old = p_temp;
+            q_old = q_temp;
+            qq_old = qq_temp;
+            ql_old = ql_temp;
+            delvc = delvc_temp;
+            work = 0.;
+            double vchalf;
+            compression = 1. / vnewc - 1.;
+            vchalf = vnewc - delvc * .5;
+            compHalfStep = 1. / vchalf - 1.;
+            if (eosvmin != 0.) {
+                if (vnewc <= eosvmin) compHalfStep = compression;
+            }
+            if (eosvmax != 0.) {
+                if (vnewc >= eosvmax) {
+                    p_old = 0.;
+                    compression = 0.;
+                    compHalfStep = 0.;
+                }
+            }
+            calc_energy(p_new, e_new, q_new, bvc, pbvc, p_old, e_old, q_old, compression,
+                        compHalfStep, vnewc, work, delvc, P.pmin, P.p_cut, P.e_cut, P.q_cut,
+                        P.emin, qq_old, ql_old, rho0, eosvmax);
+        }
+        D.p[zidx] = p_new;
+        D.e[zidx] = e_new;
+        D.q[zidx] = q_new;
+
+        // CalcSoundSpeedForElems_device, lulesh.cu:3795-3809
+        double ssTmp = (pbvc * e_new + vnewc * vnewc * bvc * p_new) / rho0;
+        if (ssTmp <= .1111111e-36)
+            ssTmp = .3333333e-18;
+        else
+            ssTmp = sqrt(ssTmp);
+        D.ss[zidx] = ssTmp;
+
+        // UpdateVolumesForElems_device, lulesh.cu:3850-3861
+        double tmpV = vnew_z;
+        if (fabs(tmpV - 1.0) < P.v_cut) tmpV = 1.0;
+        D.v[zidx] = tmpV;
+
+        // CalcTimeConstraintsForElems_kernel body, lulesh.cu:4246-4279
+        const double qqc2 = 64.0 * P.qqc * P.qqc;
+        const double vdov_tmp = vdov_z;
+        if (vdov_tmp != 0.) {
+            const double dtdvov = P.dvovmax / (fabs(vdov_tmp) + 1.e-20);
+            if (dth > dtdvov) dth = dtdvov;
+        }
+        const double ss_tmp = ssTmp;
+        const double area_tmp = D.arealg[zidx];
+        double dtf = ss_tmp * ss_tmp;
+        dtf += ((vdov_tmp < 0.) ? qqc2 * area_tmp * area_tmp * vdov_tmp * vdov_tmp : 0.);
+        dtf = area_tmp / sqrt(dtf);
+        if (vdov_tmp != 0. && dtf < dtc) dtc = dtf;
+    }
+    // block minimum (exact, order-free), one atomic per block
+    __shared__ double s_c[kElemBlock / 32], s_h[kElemBlock / 32];
+    dtc = warp_min(dtc);
+    dth = warp_min(dth);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        s_c[warp] = dtc;
+        s_h[warp] = dth;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double c = s_c[0], h = s_h[0];
+#pragma unroll
+        for (int w = 1; w < kElemBlock / 32; ++w) {
+            c = fmin(c, s_c[w]);
+            h = fmin(h, s_h[w]);
+        }
+        if (c < 1.0e+20) atomicMin(&T.min_courant, dbits(c));
+        if (h < 1.0e+20) atomicMin(&T.min_hydro, dbits(h));
+    }
+}
+
+void launch_eos(const SetArgs &a, int nblocks, Params P, cudaStream_t s)
+{
+    k_eos<<<nblocks, kElemBlock, 0, s>>>(a, P);
+}
+
+// ---------------------------------------------------------------------------
+// fused halo kernels of a subdomain set
+
+// CommSyncPosVel semantics (lulesh-comms-gpu.cu:1231-1661): a node shared by
+// several subdomains takes x,y,z,xd,yd,zd from the subdomain that holds it
+// on its minimum faces only (the "+side owner"), which never writes it here.
+__global__ void k_posvel_sync(SetArgs a)
+{
+    const int2 blk = a.blocks[blockIdx.x];
+    const DomDev &D = a.doms[blk.x];
+    const TimeCtl &T = a.tcs[D.tc];
+    if (!T.active) return;
+    const int i = blk.y + threadIdx.x;
+    if (i >= D.numNode) return;
+    const int en = D.en, nx = D.nx, tp = D.tp;
+    const int px = i % en, t = i / en, py = t % en, pz = t / en;
+    const int sx = (px == nx && D.col < tp - 1) ? 1 : 0;
+    const int sy = (py == nx && D.row < tp - 1) ? 1 : 0;
+    const int sz = (pz == nx && D.plane < tp - 1) ? 1 : 0;
+    if ((sx | sy | sz) == 0) return;
+    const int nb = D.nbr[(sx + 1) + 3 * (sy + 1) + 9 * (sz + 1)];
+    if (nb < 0) return;
+    const DomDev &O = a.doms[nb];
+    const int j = ((pz - sz * nx) * en + (py - sy * nx)) * en + (px - sx * nx);
+    D.x[i] = O.x[j];
+    D.y[i] = O.y[j];
+    D.z[i] = O.z[j];
+    D.xd[i] = O.xd[j];
+    D.yd[i] = O.yd[j];
+    D.zd[i] = O.zd[j];
+}
+
+void launch_posvel_sync(const SetArgs &a, int nblocks, cudaStream_t s)
+{
+    k_posvel_sync<<<nblocks, kNodeBlock, 0, s>>>(a);
+}
+
+// CommMonoQ semantics (lulesh-comms-gpu.cu:1665-1806): the delv_* ghost
+// faces (offsets of SetupConnectivityBC, lulesh.cu:581-615) receive the
+// neighbour's boundary element layer.  Block b covers face blocks[b].y>>24
+// of domain blocks[b].x, items (blocks[b].y & 0xffffff) onward.
+__global__ void k_monoq_ghost(SetArgs a)
+{
+    const int2 blk = a.blocks[blockIdx.x];
+    const DomDev &D = a.doms[blk.x];
+    const TimeCtl &T = a.tcs[D.tc];
+    if (!T.active) return;
+    const int f = blk.y >> 24;
+    const int item = (blk.y & 0xffffff) + threadIdx.x;
+    const int nx = D.nx;
+    if (item >= nx * nx || D.ghost[f] < 0) return;
+    const int a0 = item / nx, b0 = item % nx;  // (plane|row, row|col) of the face
+    int dxn = 0, dyn = 0, dzn = 0, src;
+    switch (f) {
+        case 0: dzn = -1; src = ((nx - 1) * nx + a0) * nx + b0; break;  // row a0, col b0
+        case 1: dzn = 1; src = (0 * nx + a0) * nx + b0; break;
+        case 2: dyn = -1; src = (a0 * nx + (nx - 1)) * nx + b0; break;  // plane a0, col b0
+        case 3: dyn = 1; src = (a0 * nx + 0) * nx + b0; break;
+        case 4: dxn = -1; src = (a0 * nx + b0) * nx + (nx - 1); break;  // plane a0, row b0
+        default: dxn = 1; src = (a0 * nx + b0) * nx + 0; break;
+    }
+    const int nb = D.nbr[(dxn + 1) + 3 * (dyn + 1) + 9 * (dzn + 1)];
+    if (nb < 0) return;
+    const DomDev &N = a.doms[nb];
+    const int g = D.ghost[f] + item;
+    D.delv_xi[g] = N.delv_xi[src];
+    D.delv_eta[g] = N.delv_eta[src];
+    D.delv_zeta[g] = N.delv_zeta[src];
+}
+
+void launch_monoq_ghost(const SetArgs &a, int nblocks, cudaStream_t s)
+{
+    k_monoq_ghost<<<nblocks, kElemBlock, 0, s>>>(a);
+}
+
+}  // namespace lulesh

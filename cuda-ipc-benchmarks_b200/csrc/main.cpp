@@ -1,0 +1,182 @@
+// main.cpp -- lulesh_b200 command line.
+//
+// Accepts both forms of the reference command line:
+//   CUDA form  lulesh -s N [x ITERS]       (LULESH/cuda/src/lulesh.cu:4754-4770;
+//              a 4th positional argument is the iteration count, so both
+//              "-s 45 -i 100" and the harness form "-s 45 0 200" work)
+//   omp form   -s -i -r -b -c -p -q -f -v -z -h (LULESH/omp_4.0/lulesh-util.cc:60-173)
+// plus -t TP (run as TP^3 in-device subdomains, the reference's TP^3-rank
+// run) and --staged (exchange halos through the CommSend/CommSBN/... message
+// sequence instead of the fused direct kernels), --mixed, --no-xyz.
+// Prints the report of VerifyAndWriteFinalOutput (lulesh.cu:4670-4750) with
+// the same lines and field positions, plus a full-precision energy line
+// and the true zone-cycles/s.
+#include <cuda_runtime.h>
+#include <sys/time.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+#include "lulesh.hpp"
+
+using namespace lulesh_b200;
+
+static void usage(const char *exe)
+{
+    std::printf("Usage: %s [opts]\n", exe);
+    std::printf(" where [opts] is one or more of:\n");
+    std::printf(" -q              : quiet mode - suppress all stdout\n");
+    std::printf(" -i <iterations> : number of cycles to run\n");
+    std::printf(" -s <size>       : length of cube mesh along side\n");
+    std::printf(" -r <numregions> : Number of distinct regions (def: 11)\n");
+    std::printf(" -b <balance>    : Load balance between regions of a domain (def: 1)\n");
+    std::printf(" -c <cost>       : Extra cost of more expensive regions (def: 1)\n");
+    std::printf(" -p              : Print out progress\n");
+    std::printf(" -t <tp>         : run as tp^3 subdomains on this GPU (def: 1)\n");
+    std::printf(" --staged        : halo exchange through CommSend/CommSBN messages\n");
+    std::printf(" --mixed         : FP32 element arithmetic, FP64 EOS/integration/dt\n");
+    std::printf(" --no-xyz        : do not write xyz.asc\n");
+    std::printf(" -h              : This message\n");
+    std::printf("Unstructured meshes (-u) are not supported by this build.\n");
+}
+
+static bool to_int(const char *s, int *v)
+{
+    if (!s) return false;
+    char *end = nullptr;
+    long x = std::strtol(s, &end, 10);
+    if (end == s || (*end != '\0' && *end != ' ')) return false;
+    *v = (int)x;
+    return true;
+}
+
+static double wall()
+{
+    timeval t;
+    gettimeofday(&t, nullptr);
+    return t.tv_sec + t.tv_usec * 1e-6;
+}
+
+int main(int argc, char *argv[])
+{
+    int nx = 30, its = -1, nr = 11, balance = 1, cost = 1, tp = 1;
+    bool quiet = false, progress = false, staged = false, mixed = false, xyz = true;
+    if (argc >= 2 && std::strcmp(argv[1], "-u") == 0) {
+        std::printf("Unstructured mesh input (-u) is not supported by this build\n");
+        return LFileError;
+    }
+    // CUDA form: exactly "-s N x ITERS" (argc == 5, argv[4] the count)
+    bool cuda_form = (argc == 5 && std::strcmp(argv[1], "-s") == 0 &&
+                      std::strcmp(argv[3], "-i") != 0 && argv[3][0] != '-');
+    if (cuda_form) {
+        if (!to_int(argv[2], &nx) || !to_int(argv[4], &its)) {
+            usage(argv[0]);
+            return LFileError;
+        }
+    } else {
+        for (int i = 1; i < argc; ++i) {
+            const std::string a = argv[i];
+            auto need = [&](int *dst) {
+                if (i + 1 >= argc || !to_int(argv[i + 1], dst)) {
+                    std::printf("Parse Error on option %s integer value required after argument\n",
+                                a.c_str());
+                    std::exit(-1);
+                }
+                ++i;
+            };
+            if (a == "-s") need(&nx);
+            else if (a == "-i") need(&its);
+            else if (a == "-r") need(&nr);
+            else if (a == "-b") need(&balance);
+            else if (a == "-c") need(&cost);
+            else if (a == "-t") need(&tp);
+            else if (a == "-f") { int dummy; need(&dummy); }
+            else if (a == "-z") { int dummy; need(&dummy); its = 1; }
+            else if (a == "-p") progress = true;
+            else if (a == "-q") quiet = true;
+            else if (a == "-v") {
+                std::printf("Use of -v requires compiling with -DVIZ_MESH\n");
+                return -1;
+            }
+            else if (a == "--staged") staged = true;
+            else if (a == "--mixed") mixed = true;
+            else if (a == "--no-xyz") xyz = false;
+            else if (a == "-h") { usage(argv[0]); return 0; }
+            else {
+                usage(argv[0]);
+                std::printf("ERROR: Unknown command line argument: %s\n", a.c_str());
+                return -1;
+            }
+        }
+    }
+    if (its == 0) its = -1;  // "-s N 0 ITERS": 0 means no cap in that slot
+    int flags = (staged ? LULESH_FLAG_COMM_STAGED : 0) | (mixed ? LULESH_FLAG_MIXED : 0);
+    try {
+        DomainSet set(nx, tp, nr, balance, cost, its, flags);
+        Domain origin(set, 0);
+        const int ranks = tp * tp * tp;
+        if (!quiet)
+            std::printf("Running until t=%f, Problem size=%dx%dx%d\n", 1.0e-2, nx * tp, nx * tp,
+                        nx * tp);
+        cudaDeviceSynchronize();
+        const double t0 = wall();
+        int st = LULESH_OK;
+        if (progress) {
+            lulesh_job_state s;
+            st = lulesh_host_cycle(set.get(), nullptr, &s);
+            while (st == LULESH_OK && !s.done) {
+                if (!quiet)
+                    std::printf("cycle = %d, time = %e, dt=%e\n", s.cycle, s.time, s.deltatime);
+                st = lulesh_host_cycle(set.get(), nullptr, &s);
+            }
+        } else {
+            st = lulesh_run(set.get(), 256);
+        }
+        cudaDeviceSynchronize();
+        const double elapsed = wall() - t0;
+        lulesh_job_state s;
+        check(lulesh_job_state_get(set.get(), 0, &s), "state");
+        if (s.status == LULESH_VOLUME_ERROR) {
+            std::printf("Rank %i: Volume Error in cell %d at iteration %d\n", 0, s.bad_elem,
+                        s.cycle - 1);
+            return VolumeError;
+        }
+        if (s.status == LULESH_QSTOP_ERROR) {
+            std::printf("Rank %i: Q Error in cell %d at iteration %d\n", 0, s.bad_elem, s.cycle - 1);
+            return QStopError;
+        }
+        if (st != LULESH_OK) throw Error(st, "run");
+        if (quiet) return 0;
+        size_t free_mem = 0, total_mem = 0;
+        cudaMemGetInfo(&free_mem, &total_mem);
+        std::printf("   Used Memory         =  %8.4f Mb\n", (total_mem - free_mem) / (1024. * 1024.));
+        const int cyc = s.cycle;
+        const double grind1 = ((elapsed * 1e6) / cyc) / ((double)nx * nx * nx);
+        const double grind2 = ((elapsed * 1e6) / cyc) / ((double)nx * nx * nx * ranks);
+        double e0 = 0.0, ma = 0.0, ta = 0.0, mr = 0.0;
+        check(lulesh_origin_energy(set.get(), 0, &e0), "energy");
+        check(lulesh_symmetry(set.get(), 0, &ma, &ta, &mr), "symmetry");
+        std::printf("Run completed:  \n");
+        std::printf("   Problem size        =  %i \n", nx);
+        std::printf("   MPI tasks           =  %i \n", ranks);
+        std::printf("   Iteration count     =  %i \n", cyc);
+        std::printf("   Final Origin Energy = %12.6e \n", e0);
+        std::printf("   Testing Plane 0 of Energy Array on rank 0:\n");
+        std::printf("        MaxAbsDiff   = %12.6e\n", ma);
+        std::printf("        TotalAbsDiff = %12.6e\n", ta);
+        std::printf("        MaxRelDiff   = %12.6e\n\n", mr);
+        std::printf("\nElapsed time         = %10.2f (s)\n", elapsed);
+        std::printf("Grind time (us/z/c)  = %10.8g (per dom)  (%10.8g overall)\n", grind1, grind2);
+        // the reference prints 1000/grind (zones per ms), kept for its parsers
+        std::printf("FOM                  = %10.8g (z/s)\n\n", 1000.0 / grind2);
+        std::printf("Final Origin Energy (full precision) = %.17e\n", e0);
+        std::printf("Zone-cycles per second = %.6e\n", 1e6 / grind2);
+        if (xyz) check(lulesh_write_solution(set.get(), 0, "xyz.asc"), "write_solution");
+    } catch (const Error &e) {
+        std::fprintf(stderr, "%s\n", e.what());
+        return e.status == LULESH_INVALID_ARG ? LFileError : 1;
+    }
+    return 0;
+}

@@ -1,0 +1,892 @@
+// set.cu -- lifetime, stepping and results of a lulesh_set (the C ABI).
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "set.hpp"
+
+namespace lulesh {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+int cuda_status(cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess) return LULESH_OK;
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    if (e == cudaErrorMemoryAllocation) return LULESH_OOM;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return LULESH_NO_DEVICE;
+    return LULESH_CUDA_ERROR;
+}
+
+#define LCHECK(call)                                            \
+    do {                                                        \
+        int _st = cuda_status((call), #call);                   \
+        if (_st != LULESH_OK) return _st;                       \
+    } while (0)
+
+// ---- arena sizing ---------------------------------------------------------
+
+struct DomSizes {
+    size_t E, N, Ep, allElem, corner, en2, nr, comm;
+};
+
+static DomSizes sizes_of(int nx, int numReg, long comm_doubles)
+{
+    DomSizes s;
+    s.E = (size_t)nx * nx * nx;
+    s.N = (size_t)(nx + 1) * (nx + 1) * (nx + 1);
+    s.Ep = ((s.E + 31) / 32) * 32;
+    s.allElem = s.E + 6 * (size_t)nx * nx;
+    s.corner = 8 * s.E;
+    s.en2 = (size_t)(nx + 1) * (nx + 1);
+    s.nr = (size_t)numReg;
+    s.comm = (size_t)comm_doubles;
+    return s;
+}
+
+static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+static size_t domain_bytes(const DomSizes &s, bool mixed)
+{
+    size_t b = 0;
+    b += 16 * align256(8 * s.E);        // element doubles incl. vnew, delx_*
+    b += 3 * align256(8 * s.allElem);   // delv_* with ghost faces
+    b += 13 * align256(8 * s.N);        // node doubles
+    b += 3 * align256(8 * 8 * s.Ep);    // corner forces
+    b += align256(4 * 8 * s.Ep);        // nodelist
+    b += 10 * align256(4 * s.E);        // l*, elemBC, matElemlist, regNumList, regElemlist
+    b += 2 * align256(4 * s.N);         // nodeElemCount/Start
+    b += align256(4 * s.corner);        // nodeElemCornerList
+    b += 3 * align256(4 * s.en2);       // symm*
+    b += 3 * align256(4 * s.nr);        // regCSR, regReps, regSorted
+    if (s.comm) b += align256(8 * s.comm);
+    if (mixed) b += 3 * align256(4 * 8 * s.Ep);
+    return b;
+}
+
+// receive-buffer capacity of SetupCommBuffers, lulesh.cu:457-510, for a
+// domain with all 26 neighbours (the worst case every rank is sized for)
+static long comm_buffer_doubles(int nx, int tp)
+{
+    if (tp <= 1) return 0;
+    const long pad = 16;  // CACHE_COHERENCE_PAD_REAL for doubles
+    long maxEdge = nx + 1;
+    long maxPlane = ((maxEdge * maxEdge + pad - 1) / pad) * pad;
+    maxEdge = ((maxEdge + pad - 1) / pad) * pad;
+    (void)maxEdge;
+    return 6 * maxPlane * 6 + 12 * maxPlane * 6 + 8 * pad;
+}
+
+// ---- device helpers ----------------------------------------------------------
+
+struct Carver {
+    char *base;
+    size_t off = 0;
+    template <typename T> T *take(size_t count)
+    {
+        T *p = reinterpret_cast<T *>(base + off);
+        off += align256(sizeof(T) * count);
+        return p;
+    }
+};
+
+template <typename T>
+static int upload(T *dst, const std::vector<T> &src, cudaStream_t s)
+{
+    if (src.empty()) return LULESH_OK;
+    return cuda_status(cudaMemcpyAsync(dst, src.data(), sizeof(T) * src.size(),
+                                       cudaMemcpyHostToDevice, s),
+                       "upload");
+}
+
+static unsigned long long dbl_bits(double v)
+{
+    unsigned long long u;
+    std::memcpy(&u, &v, sizeof u);
+    return u;
+}
+
+// ---- creation -------------------------------------------------------------
+
+static int validate_job(const lulesh_job &j)
+{
+    if (j.nx < 1 || j.nx > 1024 || j.numReg < 1 || j.numReg > 1000 || j.balance < 0 ||
+        j.balance > 30 || j.cost < 0 || j.cost > 1000) {
+        set_error("invalid job parameters (nx in [1,1024], numReg >= 1, balance/cost >= 0)");
+        return LULESH_INVALID_ARG;
+    }
+    return LULESH_OK;
+}
+
+static int build_tables(lulesh_set *s)
+{
+    std::vector<int2> eb, nb, gb;
+    for (int d = 0; d < s->ndom; ++d) {
+        const DomDev &D = s->hdoms[d];
+        for (int i = 0; i < D.numElem; i += kElemBlock) eb.push_back(make_int2(d, i));
+        for (int i = 0; i < D.numNode; i += kNodeBlock) nb.push_back(make_int2(d, i));
+        if (D.tp > 1)
+            for (int f = 0; f < 6; ++f)
+                if (D.ghost[f] >= 0)
+                    for (int i = 0; i < D.nx * D.nx; i += kElemBlock)
+                        gb.push_back(make_int2(d, (f << 24) | i));
+    }
+    s->n_elem_blocks = (int)eb.size();
+    s->n_node_blocks = (int)nb.size();
+    s->n_ghost_blocks = (int)gb.size();
+    size_t bytes = sizeof(int2) * (eb.size() + nb.size() + gb.size() + 1);
+    int2 *t = nullptr;
+    LCHECK(cudaMalloc(&t, bytes));
+    s->elem_blocks = t;
+    s->node_blocks = t + eb.size();
+    s->ghost_blocks = t + eb.size() + nb.size();
+    LCHECK(cudaMemcpyAsync(s->elem_blocks, eb.data(), sizeof(int2) * eb.size(),
+                           cudaMemcpyHostToDevice, s->stream));
+    LCHECK(cudaMemcpyAsync(s->node_blocks, nb.data(), sizeof(int2) * nb.size(),
+                           cudaMemcpyHostToDevice, s->stream));
+    if (!gb.empty())
+        LCHECK(cudaMemcpyAsync(s->ghost_blocks, gb.data(), sizeof(int2) * gb.size(),
+                               cudaMemcpyHostToDevice, s->stream));
+    return LULESH_OK;
+}
+
+// Fill the arena for every domain.  `layout[d]` gives (job, tp, col, row,
+// plane, rank) of domain d.
+struct DomPlace {
+    int job, tp, col, row, plane, rank;
+};
+
+static int create_common(lulesh_set *s, const std::vector<DomPlace> &place, int device)
+{
+    if (device >= 0) LCHECK(cudaSetDevice(device));
+    LCHECK(cudaGetDevice(&s->device));
+    if (!s->stream) {
+        LCHECK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+        s->own_stream = true;
+    }
+    s->P = default_params();
+    s->ndom = (int)place.size();
+    const bool mixed = (s->flags & LULESH_FLAG_MIXED) != 0;
+
+    // arena
+    size_t total = 0;
+    std::vector<long> commd(s->ndom);
+    for (int d = 0; d < s->ndom; ++d) {
+        const lulesh_job &j = s->jobs[place[d].job];
+        commd[d] = comm_buffer_doubles(j.nx, place[d].tp);
+        total += domain_bytes(sizes_of(j.nx, j.numReg, commd[d]), mixed);
+    }
+    s->arena_bytes = total;
+    LCHECK(cudaMalloc(&s->arena, total));
+    if (mixed) LCHECK(cudaMalloc(&s->dcorner32, sizeof(CornerF32) * s->ndom));
+
+    Carver cv{static_cast<char *>(s->arena)};
+    s->hdoms.resize(s->ndom);
+    s->dom_rank.resize(s->ndom);
+    s->dom_job.resize(s->ndom);
+    s->job_origin.assign(s->njobs, -1);
+    std::vector<CornerF32> hc32(s->ndom);
+    std::vector<double> job_dt(s->njobs, 0.0);
+
+    for (int d = 0; d < s->ndom; ++d) {
+        const DomPlace &pl = place[d];
+        const lulesh_job &j = s->jobs[pl.job];
+        HostDomain h;
+        build_domain(h, j.nx, pl.tp, pl.col, pl.row, pl.plane, pl.rank, j.numReg, j.balance,
+                     j.cost, /*global_mass=*/pl.tp > 1);
+        DomSizes z = sizes_of(j.nx, j.numReg, commd[d]);
+        DomDev D{};
+        D.nx = j.nx;
+        D.en = j.nx + 1;
+        D.numElem = h.numElem;
+        D.numNode = h.numNode;
+        D.Ep = h.Ep;
+        D.allElem = h.allElem;
+        D.col = pl.col;
+        D.row = pl.row;
+        D.plane = pl.plane;
+        D.tp = pl.tp;
+        D.tc = pl.job;
+        D.numReg = j.numReg;
+        D.numSymmX = h.numSymmX;
+        D.numSymmY = h.numSymmY;
+        D.numSymmZ = h.numSymmZ;
+        for (int f = 0; f < 6; ++f) D.ghost[f] = h.ghost[f];
+        for (int k = 0; k < 27; ++k) D.nbr[k] = -1;
+        // element doubles
+        D.e = cv.take<double>(z.E); D.p = cv.take<double>(z.E); D.q = cv.take<double>(z.E);
+        D.ql = cv.take<double>(z.E); D.qq = cv.take<double>(z.E); D.v = cv.take<double>(z.E);
+        D.volo = cv.take<double>(z.E); D.delv = cv.take<double>(z.E);
+        D.vdov = cv.take<double>(z.E); D.arealg = cv.take<double>(z.E);
+        D.ss = cv.take<double>(z.E); D.elemMass = cv.take<double>(z.E);
+        D.vnew = cv.take<double>(z.E); D.delx_xi = cv.take<double>(z.E);
+        D.delx_eta = cv.take<double>(z.E); D.delx_zeta = cv.take<double>(z.E);
+        D.delv_xi = cv.take<double>(z.allElem); D.delv_eta = cv.take<double>(z.allElem);
+        D.delv_zeta = cv.take<double>(z.allElem);
+        // node doubles
+        D.x = cv.take<double>(z.N); D.y = cv.take<double>(z.N); D.z = cv.take<double>(z.N);
+        D.xd = cv.take<double>(z.N); D.yd = cv.take<double>(z.N); D.zd = cv.take<double>(z.N);
+        D.xdd = cv.take<double>(z.N); D.ydd = cv.take<double>(z.N); D.zdd = cv.take<double>(z.N);
+        D.fx = cv.take<double>(z.N); D.fy = cv.take<double>(z.N); D.fz = cv.take<double>(z.N);
+        D.nodalMass = cv.take<double>(z.N);
+        D.fx_elem = cv.take<double>(8 * z.Ep); D.fy_elem = cv.take<double>(8 * z.Ep);
+        D.fz_elem = cv.take<double>(8 * z.Ep);
+        // ints
+        D.nodelist = cv.take<int>(8 * z.Ep);
+        D.lxim = cv.take<int>(z.E); D.lxip = cv.take<int>(z.E); D.letam = cv.take<int>(z.E);
+        D.letap = cv.take<int>(z.E); D.lzetam = cv.take<int>(z.E); D.lzetap = cv.take<int>(z.E);
+        D.elemBC = cv.take<int>(z.E); D.matElemlist = cv.take<int>(z.E);
+        D.regNumList = cv.take<int>(z.E); D.regElemlist = cv.take<int>(z.E);
+        D.nodeElemCount = cv.take<int>(z.N); D.nodeElemStart = cv.take<int>(z.N);
+        D.nodeElemCornerList = cv.take<int>(z.corner);
+        D.symmX = cv.take<int>(z.en2); D.symmY = cv.take<int>(z.en2); D.symmZ = cv.take<int>(z.en2);
+        D.regCSR = cv.take<int>(z.nr); D.regReps = cv.take<int>(z.nr); D.regSorted = cv.take<int>(z.nr);
+        if (z.comm) {
+            D.commRecv = cv.take<double>(z.comm);
+            D.commRecvLen = (long)z.comm;
+        }
+        if (mixed) {
+            CornerF32 &c = hc32[d];
+            c.fx = cv.take<float>(8 * z.Ep); c.fy = cv.take<float>(8 * z.Ep);
+            c.fz = cv.take<float>(8 * z.Ep);
+        }
+
+        // upload (InitializeFields: zeros except v = 1, lulesh.cu:432-451)
+        cudaStream_t st = s->stream;
+        const size_t E = z.E, N = z.N;
+        double *edbl[16] = {D.e, D.p, D.q, D.ql, D.qq, D.v, D.volo, D.delv, D.vdov,
+                            D.arealg, D.ss, D.elemMass, D.vnew, D.delx_xi, D.delx_eta,
+                            D.delx_zeta};
+        for (double *p : edbl) LCHECK(cudaMemsetAsync(p, 0, 8 * E, st));
+        double *ndbl[13] = {D.x, D.y, D.z, D.xd, D.yd, D.zd, D.xdd, D.ydd, D.zdd,
+                            D.fx, D.fy, D.fz, D.nodalMass};
+        for (double *p : ndbl) LCHECK(cudaMemsetAsync(p, 0, 8 * N, st));
+        LCHECK(cudaMemsetAsync(D.delv_xi, 0, 8 * z.allElem, st));
+        LCHECK(cudaMemsetAsync(D.delv_eta, 0, 8 * z.allElem, st));
+        LCHECK(cudaMemsetAsync(D.delv_zeta, 0, 8 * z.allElem, st));
+        LCHECK(cudaMemsetAsync(D.fx_elem, 0, 8 * 8 * z.Ep, st));
+        LCHECK(cudaMemsetAsync(D.fy_elem, 0, 8 * 8 * z.Ep, st));
+        LCHECK(cudaMemsetAsync(D.fz_elem, 0, 8 * 8 * z.Ep, st));
+        if (z.comm) LCHECK(cudaMemsetAsync(D.commRecv, 0, 8 * z.comm, st));
+        std::vector<double> ones(E, 1.0);
+        int st_up;
+        if ((st_up = upload(D.v, ones, st)) != LULESH_OK) return st_up;
+        if ((st_up = upload(D.e, h.e, st)) != LULESH_OK) return st_up;
+        if ((st_up = upload(D.volo, h.volo, st)) != LULESH_OK) return st_up;
+        if ((st_up = upload(D.elemMass, h.elemMass, st)) != LULESH_OK) return st_up;
+        if ((st_up = upload(D.x, h.x, st)) != LULESH_OK) return st_up;
+        if ((st_up = upload(D.y, h.y, st)) != LULESH_OK) return st_up;
+        if ((st_up = upload(D.z, h.z, st)) != LULESH_OK) return st_up;
+        if ((st_up = upload(D.nodalMass, h.nodalMass, st)) != LULESH_OK) return st_up;
+        if ((st_up = upload(D.nodelist, h.nodelist, st)) != LULESH_OK) return st_up;
+        const std::vector<int> *iv[] = {&h.lxim, &h.lxip, &h.letam, &h.letap, &h.lzetam,
+                                        &h.lzetap, &h.elemBC, &h.matElemlist, &h.regNumList,
+                                        &h.regElemlist, &h.nodeElemCount, &h.nodeElemStart,
+                                        &h.nodeElemCornerList, &h.symmX, &h.symmY, &h.symmZ,
+                                        &h.regCSR, &h.regReps, &h.regSorted};
+        int *ip[] = {D.lxim, D.lxip, D.letam, D.letap, D.lzetam, D.lzetap, D.elemBC,
+                     D.matElemlist, D.regNumList, D.regElemlist, D.nodeElemCount,
+                     D.nodeElemStart, D.nodeElemCornerList, D.symmX, D.symmY, D.symmZ,
+                     D.regCSR, D.regReps, D.regSorted};
+        for (size_t k = 0; k < sizeof(ip) / sizeof(ip[0]); ++k)
+            if ((st_up = upload(ip[k], *iv[k], st)) != LULESH_OK) return st_up;
+        // host vectors must outlive the async copies
+        LCHECK(cudaStreamSynchronize(st));
+
+        s->hdoms[d] = D;
+        s->dom_rank[d] = pl.rank;
+        s->dom_job[d] = pl.job;
+        if (pl.col == 0 && pl.row == 0 && pl.plane == 0) {
+            s->job_origin[pl.job] = d;
+            job_dt[pl.job] = h.deltatime;  // the origin domain's initial dt
+        }
+    }
+    // neighbour tables of subdomain sets (rank = col + tp*(row + tp*plane))
+    for (int d = 0; d < s->ndom; ++d) {
+        DomDev &D = s->hdoms[d];
+        if (D.tp <= 1) continue;
+        const int base = d - s->dom_rank[d];
+        for (int dz = -1; dz <= 1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int c = D.col + dx, r = D.row + dy, p = D.plane + dz;
+                    int nbr = -1;
+                    if (c >= 0 && r >= 0 && p >= 0 && c < D.tp && r < D.tp && p < D.tp &&
+                        !(dx == 0 && dy == 0 && dz == 0))
+                        nbr = base + c + D.tp * (r + D.tp * p);
+                    D.nbr[(dx + 1) + 3 * (dy + 1) + 9 * (dz + 1)] = nbr;
+                }
+    }
+    LCHECK(cudaMalloc(&s->ddoms, sizeof(DomDev) * s->ndom));
+    LCHECK(cudaMemcpyAsync(s->ddoms, s->hdoms.data(), sizeof(DomDev) * s->ndom,
+                           cudaMemcpyHostToDevice, s->stream));
+    if (mixed)
+        LCHECK(cudaMemcpyAsync(s->dcorner32, hc32.data(), sizeof(CornerF32) * s->ndom,
+                               cudaMemcpyHostToDevice, s->stream));
+
+    // time control blocks
+    std::vector<TimeCtl> tc(s->njobs);
+    for (int j = 0; j < s->njobs; ++j) {
+        TimeCtl &T = tc[j];
+        std::memset(&T, 0, sizeof T);
+        T.time = 0.0;
+        T.deltatime = job_dt[j];
+        T.dtcourant = 1.0e+20;
+        T.dthydro = 1.0e+20;
+        T.min_courant = dbl_bits(1.0e+20);
+        T.min_hydro = dbl_bits(1.0e+20);
+        T.cycle = 0;
+        T.its_cap = s->jobs[j].its;
+        T.bad_vol = INT_MAX;
+        T.bad_q = INT_MAX;
+    }
+    LCHECK(cudaMalloc(&s->dtc, sizeof(TimeCtl) * s->njobs));
+    LCHECK(cudaMallocHost(&s->htc_pinned, sizeof(TimeCtl) * s->njobs));
+    LCHECK(cudaMemcpyAsync(s->dtc, tc.data(), sizeof(TimeCtl) * s->njobs,
+                           cudaMemcpyHostToDevice, s->stream));
+    int st = build_tables(s);
+    if (st != LULESH_OK) return st;
+    LCHECK(cudaStreamSynchronize(s->stream));
+    return LULESH_OK;
+}
+
+int enqueue_cycle(lulesh_set *s)
+{
+    if (s->flags & LULESH_FLAG_COMM_STAGED) return enqueue_cycle_staged(s);
+    cudaStream_t st = s->stream;
+    const bool mixed = (s->flags & LULESH_FLAG_MIXED) != 0;
+    launch_time_increment(s->dtc, s->njobs, s->P, st);
+    if (mixed)
+        launch_force_mixed(s->args(s->elem_blocks), s->n_elem_blocks, s->P, s->dcorner32, st);
+    else
+        launch_force(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st);
+    if (mixed)
+        launch_nodal_mixed(s->args(s->node_blocks), s->n_node_blocks, s->P, s->dcorner32, st);
+    else
+        launch_nodal(s->args(s->node_blocks), s->n_node_blocks, s->P, st);
+    if (s->tp > 1) launch_posvel_sync(s->args(s->node_blocks), s->n_node_blocks, st);
+    if (mixed)
+        launch_kinematics_mixed(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st);
+    else
+        launch_kinematics(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st);
+    if (s->tp > 1 && s->n_ghost_blocks > 0)
+        launch_monoq_ghost(s->args(s->ghost_blocks), s->n_ghost_blocks, st);
+    launch_eos(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st);
+    return cuda_status(cudaGetLastError(), "cycle launch");
+}
+
+static int ensure_graph(lulesh_set *s)
+{
+    if (s->graph_ready) return LULESH_OK;
+    if (s->flags & LULESH_FLAG_COMM_STAGED) {
+        int pst = comm_prepare(s);
+        if (pst != LULESH_OK) return pst;
+    }
+    LCHECK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    int st = enqueue_cycle(s);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+    if (st != LULESH_OK) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+    }
+    LCHECK(e);
+    s->graph = g;
+    LCHECK(cudaGraphInstantiate(&s->exec, g, 0));
+    s->graph_ready = true;
+    return LULESH_OK;
+}
+
+static void drop_graph(lulesh_set *s)
+{
+    if (s->exec) cudaGraphExecDestroy(s->exec);
+    if (s->graph) cudaGraphDestroy(s->graph);
+    s->exec = nullptr;
+    s->graph = nullptr;
+    s->graph_ready = false;
+}
+
+static int read_states(lulesh_set *s)
+{
+    LCHECK(cudaMemcpyAsync(s->htc_pinned, s->dtc, sizeof(TimeCtl) * s->njobs,
+                           cudaMemcpyDeviceToHost, s->stream));
+    LCHECK(cudaStreamSynchronize(s->stream));
+    return LULESH_OK;
+}
+
+static void fill_state(const TimeCtl &T, lulesh_job_state *o)
+{
+    o->status = T.status;
+    o->bad_elem = (T.status == -1) ? T.bad_vol : (T.status == -2 ? T.bad_q : -1);
+    if (T.status == 0 && T.bad_vol != INT_MAX) {
+        o->status = -1;
+        o->bad_elem = T.bad_vol;
+    } else if (T.status == 0 && T.bad_q != INT_MAX) {
+        o->status = -2;
+        o->bad_elem = T.bad_q;
+    }
+    o->cycle = T.cycle;
+    o->done = T.done;
+    o->time = T.time;
+    o->deltatime = T.deltatime;
+    o->dtcourant = T.dtcourant;
+    o->dthydro = T.dthydro;
+}
+
+// ---- field table ----------------------------------------------------------
+
+struct FieldRef {
+    void *ptr;
+    size_t bytes;
+};
+
+static bool field_of(const lulesh_set *s, int d, const char *name, FieldRef *out)
+{
+    const DomDev &D = s->hdoms[d];
+    const size_t E = D.numElem, N = D.numNode, Ep = D.Ep, A = D.allElem;
+    const size_t en2 = (size_t)D.en * D.en, nr = D.numReg;
+    struct Row {
+        const char *n;
+        void *p;
+        size_t b;
+    } rows[] = {
+        {"e", D.e, 8 * E}, {"p", D.p, 8 * E}, {"q", D.q, 8 * E}, {"ql", D.ql, 8 * E},
+        {"qq", D.qq, 8 * E}, {"v", D.v, 8 * E}, {"volo", D.volo, 8 * E},
+        {"delv", D.delv, 8 * E}, {"vdov", D.vdov, 8 * E}, {"arealg", D.arealg, 8 * E},
+        {"ss", D.ss, 8 * E}, {"elemMass", D.elemMass, 8 * E}, {"vnew", D.vnew, 8 * E},
+        {"delx_xi", D.delx_xi, 8 * E}, {"delx_eta", D.delx_eta, 8 * E},
+        {"delx_zeta", D.delx_zeta, 8 * E}, {"delv_xi", D.delv_xi, 8 * A},
+        {"delv_eta", D.delv_eta, 8 * A}, {"delv_zeta", D.delv_zeta, 8 * A},
+        {"x", D.x, 8 * N}, {"y", D.y, 8 * N}, {"z", D.z, 8 * N}, {"xd", D.xd, 8 * N},
+        {"yd", D.yd, 8 * N}, {"zd", D.zd, 8 * N}, {"xdd", D.xdd, 8 * N},
+        {"ydd", D.ydd, 8 * N}, {"zdd", D.zdd, 8 * N}, {"fx", D.fx, 8 * N},
+        {"fy", D.fy, 8 * N}, {"fz", D.fz, 8 * N}, {"nodalMass", D.nodalMass, 8 * N},
+        {"fx_elem", D.fx_elem, 64 * Ep}, {"fy_elem", D.fy_elem, 64 * Ep},
+        {"fz_elem", D.fz_elem, 64 * Ep}, {"nodelist", D.nodelist, 32 * Ep},
+        {"lxim", D.lxim, 4 * E}, {"lxip", D.lxip, 4 * E}, {"letam", D.letam, 4 * E},
+        {"letap", D.letap, 4 * E}, {"lzetam", D.lzetam, 4 * E}, {"lzetap", D.lzetap, 4 * E},
+        {"elemBC", D.elemBC, 4 * E}, {"matElemlist", D.matElemlist, 4 * E},
+        {"regNumList", D.regNumList, 4 * E}, {"regElemlist", D.regElemlist, 4 * E},
+        {"nodeElemCount", D.nodeElemCount, 4 * N}, {"nodeElemStart", D.nodeElemStart, 4 * N},
+        {"nodeElemCornerList", D.nodeElemCornerList, 32 * E}, {"symmX", D.symmX, 4 * en2},
+        {"symmY", D.symmY, 4 * en2}, {"symmZ", D.symmZ, 4 * en2},
+        {"regCSR", D.regCSR, 4 * nr}, {"regReps", D.regReps, 4 * nr},
+        {"regSorted", D.regSorted, 4 * nr},
+    };
+    for (const Row &r : rows)
+        if (std::strcmp(r.n, name) == 0) {
+            out->ptr = r.p;
+            out->bytes = r.b;
+            return true;
+        }
+    return false;
+}
+
+}  // namespace lulesh
+
+using namespace lulesh;
+
+// ============================================================================
+// C ABI
+
+extern "C" {
+
+const char *lulesh_last_error(void) { return g_last_error.c_str(); }
+
+const char *lulesh_status_string(int st)
+{
+    switch (st) {
+        case LULESH_OK: return "ok";
+        case LULESH_VOLUME_ERROR: return "VolumeError";
+        case LULESH_QSTOP_ERROR: return "QStopError";
+        case LULESH_FILE_ERROR: return "LFileError";
+        case LULESH_CUDA_ERROR: return "CUDA error";
+        case LULESH_INVALID_ARG: return "invalid argument";
+        case LULESH_OOM: return "out of device memory";
+        case LULESH_TIMEOUT: return "timeout";
+        case LULESH_NO_DEVICE: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+
+size_t lulesh_footprint_bytes(const lulesh_job *jobs, int njobs, int tp)
+{
+    if (!jobs || njobs <= 0 || tp < 1) return 0;
+    size_t total = 0;
+    for (int j = 0; j < njobs; ++j) {
+        const long comm = comm_buffer_doubles(jobs[j].nx, tp);
+        const size_t per = domain_bytes(sizes_of(jobs[j].nx, jobs[j].numReg, comm), false);
+        total += per * (size_t)tp * tp * tp;
+        // block tables, domain records and time control
+        const size_t E = (size_t)jobs[j].nx * jobs[j].nx * jobs[j].nx;
+        const size_t N = (size_t)(jobs[j].nx + 1) * (jobs[j].nx + 1) * (jobs[j].nx + 1);
+        total += tp * tp * tp * (8 * (E / kElemBlock + N / kNodeBlock + 2) + sizeof(DomDev)) +
+                 sizeof(TimeCtl);
+    }
+    return total;
+}
+
+int lulesh_create(const lulesh_job *job, int tp, int flags, int device, lulesh_set **out)
+{
+    if (!job || !out || tp < 1 || tp > 16) {
+        set_error("lulesh_create: bad arguments");
+        return LULESH_INVALID_ARG;
+    }
+    *out = nullptr;
+    int st = validate_job(*job);
+    if (st != LULESH_OK) return st;
+    if ((flags & LULESH_FLAG_MIXED) && tp > 1) {
+        set_error("mixed precision runs on single domains and batches");
+        return LULESH_INVALID_ARG;
+    }
+    lulesh_set *s = new lulesh_set;
+    s->flags = flags;
+    s->tp = tp;
+    s->njobs = 1;
+    s->jobs.push_back(*job);
+    std::vector<DomPlace> place;
+    const int n = tp * tp * tp;
+    for (int r = 0; r < n; ++r) {
+        // InitMeshDecomp, lulesh.cu:4653-4664 (one domain per rank)
+        place.push_back(DomPlace{0, tp, r % tp, (r / tp) % tp, r / (tp * tp), r});
+    }
+    st = create_common(s, place, device);
+    if (st != LULESH_OK) {
+        lulesh_destroy(s);
+        return st;
+    }
+    *out = s;
+    return LULESH_OK;
+}
+
+int lulesh_create_batch(const lulesh_job *jobs, int njobs, int flags, int device,
+                        lulesh_set **out)
+{
+    if (!jobs || !out || njobs < 1) {
+        set_error("lulesh_create_batch: bad arguments");
+        return LULESH_INVALID_ARG;
+    }
+    *out = nullptr;
+    for (int j = 0; j < njobs; ++j) {
+        int st = validate_job(jobs[j]);
+        if (st != LULESH_OK) return st;
+    }
+    if (flags & LULESH_FLAG_COMM_STAGED) {
+        set_error("batches have no halo exchange");
+        return LULESH_INVALID_ARG;
+    }
+    lulesh_set *s = new lulesh_set;
+    s->flags = flags;
+    s->tp = 1;
+    s->njobs = njobs;
+    s->jobs.assign(jobs, jobs + njobs);
+    std::vector<DomPlace> place;
+    for (int j = 0; j < njobs; ++j) place.push_back(DomPlace{j, 1, 0, 0, 0, 0});
+    int st = create_common(s, place, device);
+    if (st != LULESH_OK) {
+        lulesh_destroy(s);
+        return st;
+    }
+    *out = s;
+    return LULESH_OK;
+}
+
+int lulesh_destroy(lulesh_set *s)
+{
+    if (!s) return LULESH_OK;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    drop_graph(s);
+    comm_release(s);
+    if (s->elem_blocks) cudaFree(s->elem_blocks);
+    if (s->ddoms) cudaFree(s->ddoms);
+    if (s->dtc) cudaFree(s->dtc);
+    if (s->htc_pinned) cudaFreeHost(s->htc_pinned);
+    if (s->dcorner32) cudaFree(s->dcorner32);
+    if (s->arena) cudaFree(s->arena);
+    if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return LULESH_OK;
+}
+
+int lulesh_set_stream(lulesh_set *s, void *stream)
+{
+    if (!s) return LULESH_INVALID_ARG;
+    LCHECK(cudaStreamSynchronize(s->stream));
+    drop_graph(s);
+    if (s->own_stream) cudaStreamDestroy(s->stream);
+    if (stream) {
+        s->stream = static_cast<cudaStream_t>(stream);
+        s->own_stream = false;
+    } else {
+        LCHECK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+        s->own_stream = true;
+    }
+    return LULESH_OK;
+}
+
+int lulesh_lagrange_leapfrog(lulesh_set *s) { return lulesh_step(s, 1); }
+
+int lulesh_step(lulesh_set *s, int ncycles)
+{
+    if (!s || ncycles < 0) return LULESH_INVALID_ARG;
+    int st = ensure_graph(s);
+    if (st != LULESH_OK) return st;
+    for (int i = 0; i < ncycles; ++i) LCHECK(cudaGraphLaunch(s->exec, s->stream));
+    return LULESH_OK;
+}
+
+int lulesh_sync(lulesh_set *s)
+{
+    if (!s) return LULESH_INVALID_ARG;
+    LCHECK(cudaStreamSynchronize(s->stream));
+    return LULESH_OK;
+}
+
+int lulesh_run(lulesh_set *s, int check_every)
+{
+    if (!s) return LULESH_INVALID_ARG;
+    if (check_every <= 0) check_every = 64;
+    for (;;) {
+        int st = lulesh_step(s, check_every);
+        if (st != LULESH_OK) return st;
+        st = read_states(s);
+        if (st != LULESH_OK) return st;
+        bool all_done = true;
+        for (int j = 0; j < s->njobs; ++j)
+            if (!s->htc_pinned[j].done) all_done = false;
+        if (all_done) break;
+    }
+    for (int j = 0; j < s->njobs; ++j) {
+        lulesh_job_state o;
+        fill_state(s->htc_pinned[j], &o);
+        if (o.status != LULESH_OK) return o.status;
+    }
+    return LULESH_OK;
+}
+
+int lulesh_host_cycle(lulesh_set *s, const lulesh_job_state *in, lulesh_job_state *out)
+{
+    if (!s || s->njobs != 1) {
+        set_error("lulesh_host_cycle drives one job");
+        return LULESH_INVALID_ARG;
+    }
+    int st = ensure_graph(s);
+    if (st != LULESH_OK) return st;
+    if (in) {
+        // host -> device: the time state the host decided on
+        TimeCtl &T = s->htc_pinned[0];
+        T.time = in->time;
+        T.deltatime = in->deltatime;
+        LCHECK(cudaMemcpyAsync(&s->dtc[0].time, &T.time, 2 * sizeof(double),
+                               cudaMemcpyHostToDevice, s->stream));
+    }
+    LCHECK(cudaGraphLaunch(s->exec, s->stream));
+    // device -> host: the whole time-control record (dt, time, status)
+    LCHECK(cudaMemcpyAsync(s->htc_pinned, s->dtc, sizeof(TimeCtl), cudaMemcpyDeviceToHost,
+                           s->stream));
+    LCHECK(cudaStreamSynchronize(s->stream));
+    if (out) fill_state(s->htc_pinned[0], out);
+    lulesh_job_state tmp;
+    fill_state(s->htc_pinned[0], &tmp);
+    return tmp.status;
+}
+
+static const char *kPhaseNames[] = {"time_increment", "force", "nodal", "posvel_sync",
+                                    "kinematics", "monoq_ghost", "eos"};
+
+const char *lulesh_phase_name(int phase)
+{
+    if (phase < 0 || phase >= (int)(sizeof kPhaseNames / sizeof kPhaseNames[0])) return "";
+    return kPhaseNames[phase];
+}
+
+int lulesh_profile_phases(lulesh_set *s, int ncycles, double *ms_out, int *nphases)
+{
+    if (!s || !ms_out || !nphases || ncycles < 1) return LULESH_INVALID_ARG;
+    if (s->flags & LULESH_FLAG_COMM_STAGED) {
+        set_error("phase profiling covers the fused cycle");
+        return LULESH_INVALID_ARG;
+    }
+    const int np = 7;
+    cudaEvent_t ev[np + 1];
+    for (int k = 0; k <= np; ++k) LCHECK(cudaEventCreate(&ev[k]));
+    double acc[np] = {0};
+    cudaStream_t st = s->stream;
+    const bool mixed = (s->flags & LULESH_FLAG_MIXED) != 0;
+    for (int c = 0; c < ncycles; ++c) {
+        LCHECK(cudaEventRecord(ev[0], st));
+        launch_time_increment(s->dtc, s->njobs, s->P, st);
+        LCHECK(cudaEventRecord(ev[1], st));
+        if (mixed)
+            launch_force_mixed(s->args(s->elem_blocks), s->n_elem_blocks, s->P, s->dcorner32, st);
+        else
+            launch_force(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st);
+        LCHECK(cudaEventRecord(ev[2], st));
+        if (mixed)
+            launch_nodal_mixed(s->args(s->node_blocks), s->n_node_blocks, s->P, s->dcorner32, st);
+        else
+            launch_nodal(s->args(s->node_blocks), s->n_node_blocks, s->P, st);
+        LCHECK(cudaEventRecord(ev[3], st));
+        if (s->tp > 1) launch_posvel_sync(s->args(s->node_blocks), s->n_node_blocks, st);
+        LCHECK(cudaEventRecord(ev[4], st));
+        if (mixed)
+            launch_kinematics_mixed(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st);
+        else
+            launch_kinematics(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st);
+        LCHECK(cudaEventRecord(ev[5], st));
+        if (s->tp > 1 && s->n_ghost_blocks > 0)
+            launch_monoq_ghost(s->args(s->ghost_blocks), s->n_ghost_blocks, st);
+        LCHECK(cudaEventRecord(ev[6], st));
+        launch_eos(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st);
+        LCHECK(cudaEventRecord(ev[7], st));
+        LCHECK(cudaEventSynchronize(ev[7]));
+        for (int k = 0; k < np; ++k) {
+            float ms = 0.f;
+            LCHECK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+            acc[k] += ms;
+        }
+    }
+    for (int k = 0; k <= np; ++k) cudaEventDestroy(ev[k]);
+    for (int k = 0; k < np; ++k) ms_out[k] = acc[k] / ncycles;
+    *nphases = np;
+    return LULESH_OK;
+}
+
+int lulesh_num_jobs(const lulesh_set *s) { return s ? s->njobs : 0; }
+int lulesh_num_domains(const lulesh_set *s) { return s ? s->ndom : 0; }
+
+int lulesh_job_state_get(lulesh_set *s, int job, lulesh_job_state *out)
+{
+    if (!s || !out || job < 0 || job >= s->njobs) return LULESH_INVALID_ARG;
+    int st = read_states(s);
+    if (st != LULESH_OK) return st;
+    fill_state(s->htc_pinned[job], out);
+    return LULESH_OK;
+}
+
+int lulesh_origin_energy(lulesh_set *s, int job, double *energy)
+{
+    if (!s || !energy || job < 0 || job >= s->njobs) return LULESH_INVALID_ARG;
+    const DomDev &D = s->hdoms[s->job_origin[job]];
+    LCHECK(cudaStreamSynchronize(s->stream));
+    LCHECK(cudaMemcpy(energy, D.e, sizeof(double), cudaMemcpyDeviceToHost));
+    return LULESH_OK;
+}
+
+int lulesh_symmetry(lulesh_set *s, int job, double *max_abs, double *total_abs, double *max_rel)
+{
+    if (!s || job < 0 || job >= s->njobs) return LULESH_INVALID_ARG;
+    const DomDev &D = s->hdoms[s->job_origin[job]];
+    const int nx = D.nx;
+    std::vector<double> e((size_t)nx * nx);
+    LCHECK(cudaStreamSynchronize(s->stream));
+    LCHECK(cudaMemcpy(e.data(), D.e, sizeof(double) * e.size(), cudaMemcpyDeviceToHost));
+    double ma = 0.0, ta = 0.0, mr = 0.0;
+    for (int j = 0; j < nx; ++j)
+        for (int k = j + 1; k < nx; ++k) {
+            const double ad = std::fabs(e[j * nx + k] - e[k * nx + j]);
+            ta += ad;
+            if (ma < ad) ma = ad;
+            const double rd = ad / e[k * nx + j];
+            if (mr < rd) mr = rd;
+        }
+    if (max_abs) *max_abs = ma;
+    if (total_abs) *total_abs = ta;
+    if (max_rel) *max_rel = mr;
+    return LULESH_OK;
+}
+
+int lulesh_field_bytes(lulesh_set *s, int d, const char *name, size_t *nbytes)
+{
+    if (!s || !name || !nbytes || d < 0 || d >= s->ndom) return LULESH_INVALID_ARG;
+    FieldRef f;
+    if (!field_of(s, d, name, &f)) {
+        set_error(std::string("unknown field ") + name);
+        return LULESH_INVALID_ARG;
+    }
+    *nbytes = f.bytes;
+    return LULESH_OK;
+}
+
+int lulesh_get_field(lulesh_set *s, int d, const char *name, void *dst, size_t nbytes)
+{
+    if (!s || !name || !dst || d < 0 || d >= s->ndom) return LULESH_INVALID_ARG;
+    FieldRef f;
+    if (!field_of(s, d, name, &f) || f.bytes != nbytes) {
+        set_error(std::string("field size/name mismatch: ") + name);
+        return LULESH_INVALID_ARG;
+    }
+    LCHECK(cudaStreamSynchronize(s->stream));
+    LCHECK(cudaMemcpy(dst, f.ptr, nbytes, cudaMemcpyDeviceToHost));
+    return LULESH_OK;
+}
+
+int lulesh_set_field(lulesh_set *s, int d, const char *name, const void *src, size_t nbytes)
+{
+    if (!s || !name || !src || d < 0 || d >= s->ndom) return LULESH_INVALID_ARG;
+    FieldRef f;
+    if (!field_of(s, d, name, &f) || f.bytes != nbytes) {
+        set_error(std::string("field size/name mismatch: ") + name);
+        return LULESH_INVALID_ARG;
+    }
+    LCHECK(cudaStreamSynchronize(s->stream));
+    LCHECK(cudaMemcpy(f.ptr, src, nbytes, cudaMemcpyHostToDevice));
+    return LULESH_OK;
+}
+
+int lulesh_domain_view_get(lulesh_set *s, int d, lulesh_domain_view *o)
+{
+    if (!s || !o || d < 0 || d >= s->ndom) return LULESH_INVALID_ARG;
+    const DomDev &D = s->hdoms[d];
+    std::memset(o, 0, sizeof *o);
+    o->numElem = D.numElem;
+    o->numNode = D.numNode;
+    o->padded_numElem = D.Ep;
+    o->sizeX = o->sizeY = o->sizeZ = D.nx;
+    o->colLoc = D.col;
+    o->rowLoc = D.row;
+    o->planeLoc = D.plane;
+    o->tp = D.tp;
+    o->numReg = D.numReg;
+    o->allElem = D.allElem;
+    o->numSymmX = D.numSymmX;
+    o->numSymmY = D.numSymmY;
+    o->numSymmZ = D.numSymmZ;
+#define V(f) o->f = D.f
+    V(nodelist); V(lxim); V(lxip); V(letam); V(letap); V(lzetam); V(lzetap); V(elemBC);
+    V(nodeElemCount); V(nodeElemStart); V(nodeElemCornerList); V(symmX); V(symmY); V(symmZ);
+    V(matElemlist); V(regCSR); V(regReps); V(regNumList); V(regElemlist); V(regSorted);
+    V(e); V(p); V(q); V(ql); V(qq); V(v); V(volo); V(delv); V(vdov); V(arealg); V(ss);
+    V(elemMass); V(x); V(y); V(z); V(xd); V(yd); V(zd); V(xdd); V(ydd); V(zdd); V(fx); V(fy);
+    V(fz); V(nodalMass); V(vnew); V(delx_xi); V(delx_eta); V(delx_zeta); V(delv_xi);
+    V(delv_eta); V(delv_zeta); V(fx_elem); V(fy_elem); V(fz_elem);
+#undef V
+    return LULESH_OK;
+}
+
+int lulesh_write_solution(lulesh_set *s, int d, const char *path)
+{
+    if (!s || !path || d < 0 || d >= s->ndom) return LULESH_INVALID_ARG;
+    const DomDev &D = s->hdoms[d];
+    std::vector<double> x(D.numNode), y(D.numNode), z(D.numNode);
+    LCHECK(cudaStreamSynchronize(s->stream));
+    LCHECK(cudaMemcpy(x.data(), D.x, 8 * x.size(), cudaMemcpyDeviceToHost));
+    LCHECK(cudaMemcpy(y.data(), D.y, 8 * y.size(), cudaMemcpyDeviceToHost));
+    LCHECK(cudaMemcpy(z.data(), D.z, 8 * z.size(), cudaMemcpyDeviceToHost));
+    FILE *f = std::fopen(path, "wb");
+    if (!f) {
+        set_error(std::string("cannot open ") + path);
+        return LULESH_FILE_ERROR;
+    }
+    for (int i = 0; i < D.numNode; ++i)
+        std::fprintf(f, "%10d\n%.10f\n%.10f\n%.10f\n", i, x[i], y[i], z[i]);
+    std::fclose(f);
+    return LULESH_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,77 @@
+// set.hpp -- host-side state of a lulesh_set (one GPU, one stream).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "host_setup.hpp"
+#include "kernels.cuh"
+#include "lulesh_b200.h"
+#include "lulesh_dev.h"
+
+struct lulesh_set {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int flags = 0;
+    lulesh::Params P{};
+    int tp = 1;  // subdomains per axis of each job (1 for batches)
+    int ndom = 0, njobs = 0;
+
+    // per-domain metadata kept on the host
+    std::vector<lulesh::DomDev> hdoms;
+    std::vector<int> dom_rank;         // rank of each domain inside its job
+    std::vector<int> dom_job;          // job of each domain
+    std::vector<int> job_origin;       // domain holding the job's origin
+    std::vector<lulesh_job> jobs;
+    std::vector<size_t> corner_list_len;
+
+    // device tables
+    lulesh::DomDev *ddoms = nullptr;
+    lulesh::TimeCtl *dtc = nullptr;
+    lulesh::TimeCtl *htc_pinned = nullptr;  // pinned mirror for readback
+    int2 *elem_blocks = nullptr, *node_blocks = nullptr, *ghost_blocks = nullptr;
+    int n_elem_blocks = 0, n_node_blocks = 0, n_ghost_blocks = 0;
+
+    // mixed precision corner buffers
+    lulesh::CornerF32 *dcorner32 = nullptr;
+
+    // the arena
+    void *arena = nullptr;
+    size_t arena_bytes = 0;
+
+    // captured cycle
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool graph_ready = false;
+
+    // staged comm state: receive-buffer capacity per domain (doubles)
+    long com_buf_doubles = 0;
+    int max_plane = 0, max_edge = 0;
+    int posted_msg = 0, posted_fields = 0, posted_do_recv = 1, posted_plane_only = 0;
+
+    lulesh::SetArgs args(const int2 *blocks) const
+    {
+        lulesh::SetArgs a;
+        a.doms = ddoms;
+        a.tcs = dtc;
+        a.blocks = blocks;
+        a.materialize = (flags & LULESH_FLAG_MATERIALIZE) ? 1 : 0;
+        return a;
+    }
+};
+
+namespace lulesh {
+void set_error(const std::string &msg);
+int cuda_status(cudaError_t e, const char *what);
+// enqueue one cycle (no graph)
+int enqueue_cycle(lulesh_set *s);
+// staged comm path of one cycle (comm.cu)
+int enqueue_cycle_staged(lulesh_set *s);
+// free the comm message tables of a set (comm.cu)
+void comm_release(const lulesh_set *s);
+// allocate the staged cycle's message tables ahead of graph capture
+int comm_prepare(lulesh_set *s);
+}  // namespace lulesh

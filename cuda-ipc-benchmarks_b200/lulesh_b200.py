@@ -1,0 +1,319 @@
+"""ctypes binding of liblulesh_b200.so (include/lulesh_b200.h).
+
+The binding is a thin layer over the C ABI: every call goes to the CUDA
+library built in this directory, and a missing library raises instead of
+falling back to anything else.  Names follow the reference's Domain fields
+(LULESH/cuda/src/lulesh.h:40-298) and its command line (-s -r -b -c -i).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblulesh_b200.so")
+
+OK = 0
+VOLUME_ERROR = -1
+QSTOP_ERROR = -2
+FILE_ERROR = -3
+CUDA_ERROR = -4
+INVALID_ARG = -5
+OOM = -6
+TIMEOUT = -7
+NO_DEVICE = -8
+
+FLAG_MATERIALIZE = 0x1
+FLAG_COMM_STAGED = 0x2
+FLAG_MIXED = 0x4
+
+MSG_COMM_SBN = 1024
+MSG_SYNC_POS_VEL = 2048
+MSG_MONOQ = 3072
+
+FIELD_IDS = {
+    "x": 0, "y": 1, "z": 2, "xd": 3, "yd": 4, "zd": 5, "fx": 6, "fy": 7,
+    "fz": 8, "nodalMass": 9, "delv_xi": 10, "delv_eta": 11, "delv_zeta": 12,
+}
+
+INT_FIELDS = {
+    "nodelist", "lxim", "lxip", "letam", "letap", "lzetam", "lzetap", "elemBC",
+    "matElemlist", "regNumList", "regElemlist", "nodeElemCount",
+    "nodeElemStart", "nodeElemCornerList", "symmX", "symmY", "symmZ", "regCSR",
+    "regReps", "regSorted",
+}
+
+# every symbol include/lulesh_b200.h declares
+EXPORTED = [
+    "lulesh_create", "lulesh_create_batch", "lulesh_destroy",
+    "lulesh_footprint_bytes", "lulesh_set_stream", "lulesh_lagrange_leapfrog",
+    "lulesh_step", "lulesh_run", "lulesh_host_cycle", "lulesh_sync",
+    "lulesh_num_jobs", "lulesh_num_domains", "lulesh_job_state_get",
+    "lulesh_origin_energy", "lulesh_symmetry", "lulesh_field_bytes",
+    "lulesh_get_field", "lulesh_set_field", "lulesh_domain_view_get",
+    "lulesh_write_solution", "lulesh_status_string", "lulesh_last_error",
+    "lulesh_comm_recv", "lulesh_comm_send", "lulesh_comm_sbn",
+    "lulesh_comm_sync_posvel", "lulesh_comm_monoq", "lulesh_comm_recv_offset",
+    "lulesh_profile_phases", "lulesh_phase_name",
+]
+
+
+class Job(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("numReg", ctypes.c_int),
+                ("balance", ctypes.c_int), ("cost", ctypes.c_int),
+                ("its", ctypes.c_int)]
+
+
+class JobState(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("bad_elem", ctypes.c_int),
+                ("cycle", ctypes.c_int), ("done", ctypes.c_int),
+                ("time", ctypes.c_double), ("deltatime", ctypes.c_double),
+                ("dtcourant", ctypes.c_double), ("dthydro", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class LuleshError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{msg} (status {status})")
+        self.status = status
+
+
+_lib = None
+
+
+def load_library(path: str | None = None) -> ctypes.CDLL:
+    """Load the CUDA library; raises FileNotFoundError if it was not built."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise FileNotFoundError(
+            f"{p} is missing: build it with `make -C {HERE}` (nvcc, sm_100a)")
+    lib = ctypes.CDLL(p)
+    vp, ip, dp = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    sig = {
+        "lulesh_create": (ip, [ctypes.POINTER(Job), ip, ip, ip, ctypes.POINTER(vp)]),
+        "lulesh_create_batch": (ip, [ctypes.POINTER(Job), ip, ip, ip, ctypes.POINTER(vp)]),
+        "lulesh_destroy": (ip, [vp]),
+        "lulesh_footprint_bytes": (ctypes.c_size_t, [ctypes.POINTER(Job), ip, ip]),
+        "lulesh_set_stream": (ip, [vp, vp]),
+        "lulesh_lagrange_leapfrog": (ip, [vp]),
+        "lulesh_step": (ip, [vp, ip]),
+        "lulesh_run": (ip, [vp, ip]),
+        "lulesh_host_cycle": (ip, [vp, ctypes.POINTER(JobState), ctypes.POINTER(JobState)]),
+        "lulesh_sync": (ip, [vp]),
+        "lulesh_num_jobs": (ip, [vp]),
+        "lulesh_num_domains": (ip, [vp]),
+        "lulesh_job_state_get": (ip, [vp, ip, ctypes.POINTER(JobState)]),
+        "lulesh_origin_energy": (ip, [vp, ip, ctypes.POINTER(dp)]),
+        "lulesh_symmetry": (ip, [vp, ip, ctypes.POINTER(dp), ctypes.POINTER(dp),
+                                 ctypes.POINTER(dp)]),
+        "lulesh_field_bytes": (ip, [vp, ip, ctypes.c_char_p, ctypes.POINTER(ctypes.c_size_t)]),
+        "lulesh_get_field": (ip, [vp, ip, ctypes.c_char_p, vp, ctypes.c_size_t]),
+        "lulesh_set_field": (ip, [vp, ip, ctypes.c_char_p, vp, ctypes.c_size_t]),
+        "lulesh_domain_view_get": (ip, [vp, ip, vp]),
+        "lulesh_write_solution": (ip, [vp, ip, ctypes.c_char_p]),
+        "lulesh_status_string": (ctypes.c_char_p, [ip]),
+        "lulesh_last_error": (ctypes.c_char_p, []),
+        "lulesh_comm_recv": (ip, [vp, ip, ip, ip, ip, ip, ip, ip, ip]),
+        "lulesh_comm_send": (ip, [vp, ip, ip, ip, ctypes.POINTER(ip), ip, ip, ip, ip, ip]),
+        "lulesh_comm_sbn": (ip, [vp, ip, ip, ctypes.POINTER(ip)]),
+        "lulesh_comm_sync_posvel": (ip, [vp, ip]),
+        "lulesh_comm_monoq": (ip, [vp, ip]),
+        "lulesh_comm_recv_offset": (ctypes.c_long, [vp, ip, ip, ip, ip, ip, ip, ip]),
+        "lulesh_profile_phases": (ip, [vp, ip, ctypes.POINTER(dp), ctypes.POINTER(ip)]),
+        "lulesh_phase_name": (ctypes.c_char_p, [ip]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def _check(lib, st: int, what: str) -> int:
+    if st != OK:
+        detail = lib.lulesh_last_error().decode(errors="replace")
+        name = lib.lulesh_status_string(st).decode()
+        raise LuleshError(st, f"{what}: {name} {detail}".strip())
+    return st
+
+
+@dataclass
+class JobSpec:
+    nx: int
+    numReg: int = 11
+    balance: int = 1
+    cost: int = 1
+    its: int = -1
+
+    def c(self) -> Job:
+        return Job(self.nx, self.numReg, self.balance, self.cost, self.its)
+
+
+def footprint_bytes(jobs: list[JobSpec], tp: int = 1) -> int:
+    lib = load_library()
+    arr = (Job * len(jobs))(*[j.c() for j in jobs])
+    return int(lib.lulesh_footprint_bytes(arr, len(jobs), tp))
+
+
+class LuleshSet:
+    """One set of domains resident on one GPU (single domain, tp^3
+    subdomains, or a batch of independent jobs)."""
+
+    def __init__(self, nx: int = 30, tp: int = 1, numReg: int = 11, balance: int = 1,
+                 cost: int = 1, its: int = -1, flags: int = 0, device: int = -1,
+                 _handle=None):
+        self.lib = load_library()
+        if _handle is not None:
+            self.h = _handle
+        else:
+            h = ctypes.c_void_p()
+            job = JobSpec(nx, numReg, balance, cost, its).c()
+            _check(self.lib, self.lib.lulesh_create(ctypes.byref(job), tp, flags, device,
+                                                    ctypes.byref(h)), "lulesh_create")
+            self.h = h
+        self.tp = tp
+
+    @classmethod
+    def batch(cls, jobs: list[JobSpec], flags: int = 0, device: int = -1) -> "LuleshSet":
+        lib = load_library()
+        arr = (Job * len(jobs))(*[j.c() for j in jobs])
+        h = ctypes.c_void_p()
+        _check(lib, lib.lulesh_create_batch(arr, len(jobs), flags, device, ctypes.byref(h)),
+               "lulesh_create_batch")
+        return cls(_handle=h)
+
+    # -- lifetime
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.lulesh_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- stepping
+    def step(self, ncycles: int = 1) -> None:
+        _check(self.lib, self.lib.lulesh_step(self.h, ncycles), "lulesh_step")
+
+    def run(self, check_every: int = 64) -> int:
+        """Run to completion; returns the status (VolumeError/QStopError are
+        returned, not raised, as the reference exits with them)."""
+        st = self.lib.lulesh_run(self.h, check_every)
+        if st not in (OK, VOLUME_ERROR, QSTOP_ERROR):
+            _check(self.lib, st, "lulesh_run")
+        return st
+
+    def sync(self) -> None:
+        _check(self.lib, self.lib.lulesh_sync(self.h), "lulesh_sync")
+
+    def profile_phases(self, ncycles: int) -> dict:
+        """Average ms per phase over `ncycles` separately launched cycles."""
+        out = (ctypes.c_double * 12)()
+        n = ctypes.c_int()
+        _check(self.lib, self.lib.lulesh_profile_phases(self.h, ncycles, out, ctypes.byref(n)),
+               "lulesh_profile_phases")
+        return {self.lib.lulesh_phase_name(k).decode(): out[k] for k in range(n.value)}
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        _check(self.lib, self.lib.lulesh_set_stream(self.h, stream_ptr), "lulesh_set_stream")
+
+    def host_cycle(self, state_in: JobState | None = None) -> tuple[int, JobState]:
+        out = JobState()
+        st = self.lib.lulesh_host_cycle(self.h, ctypes.byref(state_in) if state_in else None,
+                                        ctypes.byref(out))
+        if st not in (OK, VOLUME_ERROR, QSTOP_ERROR):
+            _check(self.lib, st, "lulesh_host_cycle")
+        return st, out
+
+    # -- results
+    @property
+    def num_jobs(self) -> int:
+        return self.lib.lulesh_num_jobs(self.h)
+
+    @property
+    def num_domains(self) -> int:
+        return self.lib.lulesh_num_domains(self.h)
+
+    def state(self, job: int = 0) -> dict:
+        s = JobState()
+        _check(self.lib, self.lib.lulesh_job_state_get(self.h, job, ctypes.byref(s)),
+               "lulesh_job_state_get")
+        return s.as_dict()
+
+    def origin_energy(self, job: int = 0) -> float:
+        v = ctypes.c_double()
+        _check(self.lib, self.lib.lulesh_origin_energy(self.h, job, ctypes.byref(v)),
+               "lulesh_origin_energy")
+        return v.value
+
+    def symmetry(self, job: int = 0) -> tuple[float, float, float]:
+        a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        _check(self.lib, self.lib.lulesh_symmetry(self.h, job, ctypes.byref(a), ctypes.byref(b),
+                                                  ctypes.byref(c)), "lulesh_symmetry")
+        return a.value, b.value, c.value
+
+    def field(self, name: str, domain: int = 0) -> np.ndarray:
+        nb = ctypes.c_size_t()
+        _check(self.lib, self.lib.lulesh_field_bytes(self.h, domain, name.encode(),
+                                                     ctypes.byref(nb)), "lulesh_field_bytes")
+        dt = np.int32 if name in INT_FIELDS else np.float64
+        out = np.empty(nb.value // np.dtype(dt).itemsize, dtype=dt)
+        _check(self.lib, self.lib.lulesh_get_field(self.h, domain, name.encode(),
+                                                   out.ctypes.data_as(ctypes.c_void_p),
+                                                   nb.value), "lulesh_get_field")
+        return out
+
+    def set_field(self, name: str, values: np.ndarray, domain: int = 0) -> None:
+        dt = np.int32 if name in INT_FIELDS else np.float64
+        arr = np.ascontiguousarray(values, dtype=dt)
+        _check(self.lib, self.lib.lulesh_set_field(self.h, domain, name.encode(),
+                                                   arr.ctypes.data_as(ctypes.c_void_p),
+                                                   arr.nbytes), "lulesh_set_field")
+
+    def write_solution(self, path: str, domain: int = 0) -> None:
+        _check(self.lib, self.lib.lulesh_write_solution(self.h, domain, path.encode()),
+               "lulesh_write_solution")
+
+    # -- comm backend (rank = subdomain index, -1 = all)
+    def comm_recv(self, rank, msg, xfer, dx, dy, dz, do_recv, plane_only):
+        _check(self.lib, self.lib.lulesh_comm_recv(self.h, rank, msg, xfer, dx, dy, dz,
+                                                   int(do_recv), int(plane_only)), "CommRecv")
+
+    def comm_send(self, rank, msg, fields, dx, dy, dz, do_send, plane_only):
+        ids = (ctypes.c_int * len(fields))(*[FIELD_IDS[f] for f in fields])
+        _check(self.lib, self.lib.lulesh_comm_send(self.h, rank, msg, len(fields), ids, dx, dy,
+                                                   dz, int(do_send), int(plane_only)),
+               "CommSend")
+
+    def comm_sbn(self, rank, fields):
+        ids = (ctypes.c_int * len(fields))(*[FIELD_IDS[f] for f in fields])
+        _check(self.lib, self.lib.lulesh_comm_sbn(self.h, rank, len(fields), ids), "CommSBN")
+
+    def comm_sync_posvel(self, rank):
+        _check(self.lib, self.lib.lulesh_comm_sync_posvel(self.h, rank), "CommSyncPosVel")
+
+    def comm_monoq(self, rank):
+        _check(self.lib, self.lib.lulesh_comm_monoq(self.h, rank), "CommMonoQ")
+
+    def comm_recv_offset(self, recv_rank, dc, dr, dp, xfer, do_recv, plane_only) -> int:
+        return int(self.lib.lulesh_comm_recv_offset(self.h, recv_rank, dc, dr, dp, xfer,
+                                                    int(do_recv), int(plane_only)))

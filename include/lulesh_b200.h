@@ -1,0 +1,244 @@
+/*
+ * lulesh_b200.h -- C ABI of the B200-native LULESH Lagrange leapfrog step.
+ *
+ * Plain C types only (no CUDA or torch types): a ctypes / cgo / JNI binding
+ * can load liblulesh_b200.so and call these directly.  Every entry point
+ * returns a status code (enum lulesh_status) instead of calling exit(), and
+ * the reference's exit codes keep their values.
+ *
+ * Reference interfaces replaced (paths inside varunchotalia/cuda-ipc-benchmarks):
+ *   NewDomain                LULESH/cuda/src/lulesh.cu:750-1221
+ *   LagrangeLeapFrog         LULESH/cuda/src/lulesh.cu:4438-4452
+ *   TimeIncrement            LULESH/cuda/src/lulesh.cu:1400-1461
+ *   main loop + checkErrors  LULESH/cuda/src/lulesh.cu:4858-4873, 2879-2892
+ *   VerifyAndWriteFinalOutput LULESH/cuda/src/lulesh.cu:4670-4750
+ *   write_solution           LULESH/cuda/src/lulesh.cu:4584-4603
+ *   Domain field layout      LULESH/cuda/src/lulesh.h:40-298
+ *   CommRecv/CommSend/CommSBN/CommSyncPosVel/CommMonoQ
+ *                            LULESH/cuda/src/lulesh.h:321-340
+ *   error codes              LULESH/cuda/src/lulesh.h:22-26
+ *
+ * A "set" is everything resident on one GPU that one stream advances:
+ *   - one domain (the reference's single-rank run),
+ *   - tp^3 subdomains of one problem (the reference's tp^3-rank run, with
+ *     the halo exchange done in device memory; "rank" = subdomain index),
+ *   - or a batch of independent jobs of different sizes.
+ */
+#ifndef LULESH_B200_H
+#define LULESH_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LULESH_B200_ABI_VERSION 1
+
+/* lulesh.h:22-26 keeps -1/-2/-3; the rest are new, all negative. */
+enum lulesh_status {
+    LULESH_OK = 0,
+    LULESH_VOLUME_ERROR = -1, /* VolumeError: negative element volume   */
+    LULESH_QSTOP_ERROR = -2,  /* QStopError: q above qstop              */
+    LULESH_FILE_ERROR = -3,   /* LFileError: bad command line / input   */
+    LULESH_CUDA_ERROR = -4,   /* a CUDA runtime call failed             */
+    LULESH_INVALID_ARG = -5,  /* bad argument (size, index, name, ...)  */
+    LULESH_OOM = -6,          /* device memory exhausted / over the cap */
+    LULESH_TIMEOUT = -7,      /* a bounded device wait gave up          */
+    LULESH_NO_DEVICE = -8     /* no CUDA device / extension unusable    */
+};
+
+/* create flags */
+#define LULESH_FLAG_MATERIALIZE 0x1 /* also write the per-cycle transients the
+                                       reference keeps in Domain (fx/fy/fz,
+                                       xdd/ydd/zdd, ql/qq, vnew, delx_*,
+                                       delv_*, corner forces) every cycle   */
+#define LULESH_FLAG_COMM_STAGED 0x2 /* subdomain sets: exchange halos through
+                                       per-message buffers with the
+                                       reference's CommSend/CommSBN/
+                                       CommSyncPosVel/CommMonoQ sequence
+                                       instead of the fused direct kernels */
+#define LULESH_FLAG_MIXED 0x4       /* FP32 element-local stress/hourglass/
+                                       kinematics arithmetic, compensated
+                                       FP32 corner-force sums, FP64 EOS,
+                                       node integration and dt              */
+
+/* One sedov job: the reference command line -s -r -b -c -i
+ * (LULESH/omp_4.0/lulesh-util.cc:60-173; defaults 30/11/1/1). */
+typedef struct lulesh_job {
+    int nx;      /* -s: elements per edge of each (sub)domain, >= 1       */
+    int numReg;  /* -r: regions (cost model only), >= 1                  */
+    int balance; /* -b                                                    */
+    int cost;    /* -c                                                    */
+    int its;     /* -i: cycle cap; <= 0 runs until time >= stoptime       */
+} lulesh_job;
+
+/* Per-job progress, read back from the device. */
+typedef struct lulesh_job_state {
+    int status;    /* enum lulesh_status of this job                      */
+    int bad_elem;  /* element that raised VolumeError/QStopError, or -1   */
+    int cycle;     /* cycles completed                                    */
+    int done;      /* 1 once time >= stoptime, its reached, or an error   */
+    double time;   /* simulated time                                      */
+    double deltatime;
+    double dtcourant;
+    double dthydro;
+} lulesh_job_state;
+
+/* Device pointers of one domain, named as the Domain members of
+ * lulesh.h:40-298 (node-major nodelist with stride padded_numElem, corner
+ * index elem + padded_numElem*corner, delv_* with the ghost-face tail). */
+typedef struct lulesh_domain_view {
+    int numElem, numNode, padded_numElem, sizeX, sizeY, sizeZ;
+    int colLoc, rowLoc, planeLoc, tp, numReg, allElem;
+    int numSymmX, numSymmY, numSymmZ;
+    int *nodelist, *lxim, *lxip, *letam, *letap, *lzetam, *lzetap, *elemBC;
+    int *nodeElemCount, *nodeElemStart, *nodeElemCornerList;
+    int *symmX, *symmY, *symmZ, *matElemlist;
+    int *regCSR, *regReps, *regNumList, *regElemlist, *regSorted;
+    double *e, *p, *q, *ql, *qq, *v, *volo, *delv, *vdov, *arealg, *ss,
+        *elemMass;
+    double *x, *y, *z, *xd, *yd, *zd, *xdd, *ydd, *zdd, *fx, *fy, *fz,
+        *nodalMass;
+    double *vnew, *delx_xi, *delx_eta, *delx_zeta, *delv_xi, *delv_eta,
+        *delv_zeta, *fx_elem, *fy_elem, *fz_elem;
+} lulesh_domain_view;
+
+typedef struct lulesh_set lulesh_set;
+
+/* ---- lifetime -------------------------------------------------------- */
+
+/* Replaces NewDomain (lulesh.cu:750) for one problem decomposed into tp^3
+ * subdomains of job->nx^3 elements each (tp = 1: the single-domain run).
+ * Subdomain r sits at col = r % tp, row = (r / tp) % tp, plane = r / tp^2
+ * (InitMeshDecomp, lulesh.cu:4606-4668) and seeds its regions with
+ * srand(r) (lulesh.cu:1263-1270).  All device memory comes from one arena
+ * owned by the set.  `device` < 0 keeps the current device. */
+int lulesh_create(const lulesh_job *job, int tp, int flags, int device,
+                  lulesh_set **out);
+
+/* A batch of independent single-domain jobs advanced together; each keeps
+ * its own dt, time, cycle cap and status.  No reference counterpart: the
+ * reference runs one job per process. */
+int lulesh_create_batch(const lulesh_job *jobs, int njobs, int flags,
+                        int device, lulesh_set **out);
+
+/* Frees the arena, graphs and streams (the reference's teardown,
+ * lulesh.cu:4904-4944, minus MPI). */
+int lulesh_destroy(lulesh_set *set);
+
+/* Bytes of device memory a set of these jobs would hold (the admission
+ * model of the serving loop). */
+size_t lulesh_footprint_bytes(const lulesh_job *jobs, int njobs, int tp);
+
+/* ---- stepping -------------------------------------------------------- */
+
+/* Use this stream (a cudaStream_t passed as void*) for all later work;
+ * NULL makes the set create and own one. */
+int lulesh_set_stream(lulesh_set *set, void *stream);
+
+/* One cycle of TimeIncrement + LagrangeLeapFrog for every job in the set,
+ * enqueued asynchronously as a captured CUDA graph (lulesh.cu:4438-4452
+ * with TimeIncrement moved onto the device).  Jobs that are done skip. */
+int lulesh_lagrange_leapfrog(lulesh_set *set);
+
+/* `ncycles` such cycles, asynchronously. */
+int lulesh_step(lulesh_set *set, int ncycles);
+
+/* The reference main loop (lulesh.cu:4858-4873): cycles until every job
+ * has reached its cap or stoptime or failed, checking status every
+ * `check_every` cycles (<= 0: 64).  Synchronous.  Returns LULESH_OK or the
+ * first job error (VolumeError / QStopError as the reference's exit code). */
+int lulesh_run(lulesh_set *set, int check_every);
+
+/* One cycle driven from the host the way the reference drives it: the
+ * host passes the time state in (host buffer, copied H2D), the device runs
+ * one cycle, and the new time state plus status come back (D2H) into
+ * `out`.  in may be NULL to continue from the device state.  Used for the
+ * end-to-end measurement; synchronous. */
+int lulesh_host_cycle(lulesh_set *set, const lulesh_job_state *in,
+                      lulesh_job_state *out);
+
+/* Block until queued work is done; returns the first CUDA error seen. */
+int lulesh_sync(lulesh_set *set);
+
+/* Profiling: run `ncycles` cycles launching each phase on its own with CUDA
+ * events around it (on the set's stream), and return the average duration
+ * in milliseconds of each phase in ms_out[0..*nphases-1], named by
+ * lulesh_phase_name().  No reference counterpart (the reference times the
+ * whole loop, lulesh.cu:4851-4886). */
+int lulesh_profile_phases(lulesh_set *set, int ncycles, double *ms_out, int *nphases);
+const char *lulesh_phase_name(int phase);
+#define LULESH_MAX_PHASES 12
+
+/* ---- results --------------------------------------------------------- */
+
+int lulesh_num_jobs(const lulesh_set *set);
+int lulesh_num_domains(const lulesh_set *set);
+int lulesh_job_state_get(lulesh_set *set, int job, lulesh_job_state *out);
+
+/* e[octantCorner] of the job's origin domain (lulesh.cu:4700-4710). */
+int lulesh_origin_energy(lulesh_set *set, int job, double *energy);
+
+/* Plane-0 symmetry check of the job's origin domain (lulesh.cu:4712-4736). */
+int lulesh_symmetry(lulesh_set *set, int job, double *max_abs,
+                    double *total_abs, double *max_rel);
+
+/* Copy a named Domain field of one domain to/from host memory.  `nbytes`
+ * must equal the field's size (lulesh_field_bytes). */
+int lulesh_field_bytes(lulesh_set *set, int domain, const char *name,
+                       size_t *nbytes);
+int lulesh_get_field(lulesh_set *set, int domain, const char *name,
+                     void *host_dst, size_t nbytes);
+int lulesh_set_field(lulesh_set *set, int domain, const char *name,
+                     const void *host_src, size_t nbytes);
+
+/* Device pointers of one domain (valid until lulesh_destroy). */
+int lulesh_domain_view_get(lulesh_set *set, int domain,
+                           lulesh_domain_view *out);
+
+/* Write xyz.asc-format node coordinates of one domain (lulesh.cu:4584). */
+int lulesh_write_solution(lulesh_set *set, int domain, const char *path);
+
+const char *lulesh_status_string(int status);
+const char *lulesh_last_error(void);
+
+/* ---- comm backend (lulesh.h:321-340; comm/comm_backend.h:7-22) ------- */
+/* msgType: 1024 MSG_COMM_SBN, 2048 MSG_SYNC_POS_VEL, 3072 MSG_MONOQ
+ * (lulesh.h:314-317).  Fields are named by Domain member id below.  `rank`
+ * is a subdomain index of the set, or -1 for every subdomain in one launch.
+ * These run on the set's stream and order like the reference: all ranks'
+ * CommRecv, then CommSend, then the unpack (CommSBN / CommSyncPosVel /
+ * CommMonoQ).  A single-domain set returns LULESH_OK without work, as the
+ * reference does when numRanks() == 1 (lulesh-comms.cu:65-66). */
+enum lulesh_field_id {
+    LULESH_F_X = 0, LULESH_F_Y, LULESH_F_Z, LULESH_F_XD, LULESH_F_YD,
+    LULESH_F_ZD, LULESH_F_FX, LULESH_F_FY, LULESH_F_FZ, LULESH_F_NODALMASS,
+    LULESH_F_DELV_XI, LULESH_F_DELV_ETA, LULESH_F_DELV_ZETA
+};
+#define LULESH_MSG_COMM_SBN 1024
+#define LULESH_MSG_SYNC_POS_VEL 2048
+#define LULESH_MSG_MONOQ 3072
+#define LULESH_MAX_FIELDS_PER_COMM 6
+
+int lulesh_comm_recv(lulesh_set *set, int rank, int msgType, int xferFields,
+                     int dx, int dy, int dz, int doRecv, int planeOnly);
+int lulesh_comm_send(lulesh_set *set, int rank, int msgType, int xferFields,
+                     const int *fieldIds, int dx, int dy, int dz, int doSend,
+                     int planeOnly);
+int lulesh_comm_sbn(lulesh_set *set, int rank, int xferFields,
+                    const int *fieldIds);
+int lulesh_comm_sync_posvel(lulesh_set *set, int rank);
+int lulesh_comm_monoq(lulesh_set *set, int rank);
+
+/* Offset (in doubles) inside rank recvRank's receive buffer where the
+ * message from direction (dCol,dRow,dPlane) lands: the posting-order
+ * contract of comm_backend.h:75-138.  Returns -1 if no such message. */
+long lulesh_comm_recv_offset(lulesh_set *set, int recvRank, int dCol,
+                             int dRow, int dPlane, int xferFields, int doRecv,
+                             int planeOnly);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LULESH_B200_H */
