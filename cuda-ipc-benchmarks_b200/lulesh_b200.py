@@ -57,7 +57,7 @@ EXPORTED = [
     "lulesh_write_solution", "lulesh_status_string", "lulesh_last_error",
     "lulesh_comm_recv", "lulesh_comm_send", "lulesh_comm_sbn",
     "lulesh_comm_sync_posvel", "lulesh_comm_monoq", "lulesh_comm_recv_offset",
-    "lulesh_profile_phases", "lulesh_phase_name",
+    "lulesh_profile_phases", "lulesh_phase_name", "lulesh_volume_force_noalloc",
 ]
 
 
@@ -129,6 +129,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "lulesh_comm_recv_offset": (ctypes.c_long, [vp, ip, ip, ip, ip, ip, ip, ip]),
         "lulesh_profile_phases": (ip, [vp, ip, ctypes.POINTER(dp), ctypes.POINTER(ip)]),
         "lulesh_phase_name": (ctypes.c_char_p, [ip]),
+        "lulesh_volume_force_noalloc": (ip, [ip] + [vp] * 12 + [dp] + [vp] * 5),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

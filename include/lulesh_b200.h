@@ -203,6 +203,38 @@ int lulesh_write_solution(lulesh_set *set, int domain, const char *path);
 const char *lulesh_status_string(int status);
 const char *lulesh_last_error(void);
 
+/* ---- nodal forces without allocation --------------------------------- */
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory -- a host code whose memory manager owns the whole GPU budget, or a
+ * latency-sensitive loop that cannot afford cudaMalloc/cudaFree, which
+ * synchronise the device -- this computes the nodal forces fx/fy/fz of one
+ * structured domain of nx^3 elements (stress + FB hourglass corner forces
+ * summed per node in corner order, as CalcVolumeForceForElems does) from
+ * caller-owned device arrays in the Domain layout: x..zd over (nx+1)^3
+ * nodes, volo/v/p/q/ss/elemMass over nx^3 elements.  hgcoef is the
+ * hourglass coefficient (3.0 in the reference).  *bad_elem (device int,
+ * may be NULL) receives the smallest element with a negative volume, or -1.
+ *
+ * It allocates nothing: its only scratch is one fixed device array of
+ * LULESH_NOALLOC_MAX_ELEMS elements' corner forces (6 MiB) that every GPU
+ * which loads the library holds until the process exits.  nx above
+ * LULESH_NOALLOC_MAX_NX is rejected with LULESH_INVALID_ARG and a message in
+ * lulesh_last_error().  The first call on a device looks up that array's
+ * device address (with the device current), so make the first call on each
+ * device before any stream capture.  All calls share the one array and it
+ * keeps the last call's contents: calls that overlap on the GPU (different
+ * streams, or different host threads, on the same device) race with each
+ * other; serialise them on one stream.  Asynchronous on `stream`
+ * (a cudaStream_t, NULL for the legacy default stream). */
+#define LULESH_NOALLOC_MAX_NX 32
+#define LULESH_NOALLOC_MAX_ELEMS (LULESH_NOALLOC_MAX_NX * LULESH_NOALLOC_MAX_NX * LULESH_NOALLOC_MAX_NX)
+int lulesh_volume_force_noalloc(int nx, const double *x, const double *y, const double *z,
+                                const double *xd, const double *yd, const double *zd,
+                                const double *volo, const double *v, const double *p,
+                                const double *q, const double *ss, const double *elemMass,
+                                double hgcoef, double *fx, double *fy, double *fz,
+                                int *bad_elem, void *stream);
+
 /* ---- comm backend (lulesh.h:321-340; comm/comm_backend.h:7-22) ------- */
 /* msgType: 1024 MSG_COMM_SBN, 2048 MSG_SYNC_POS_VEL, 3072 MSG_MONOQ
  * (lulesh.h:314-317).  Fields are named by Domain member id below.  `rank`
