@@ -443,7 +443,7 @@ int enqueue_cycle_staged(lulesh_set *s)
 {
     cudaStream_t st = s->stream;
     launch_time_increment(s->dtc, s->njobs, s->P, st);
-    launch_force(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st);
+    launch_force_fp64(s, st);
     // AddNodeForcesFromElems over local corners only, then SBN exchange
     launch_nodal_gather_local(s->args(s->node_blocks), s->n_node_blocks, st);
     FieldList f3{3, {LULESH_F_FX, LULESH_F_FY, LULESH_F_FZ}};

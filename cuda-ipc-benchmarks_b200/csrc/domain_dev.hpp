@@ -1,0 +1,47 @@
+// domain_dev.hpp -- device memory of one domain: sizing, carving, upload.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+
+#include "host_setup.hpp"
+#include "lulesh_b200.h"
+#include "lulesh_dev.h"
+
+namespace lulesh {
+
+struct DomSizes {
+    size_t E, N, Ep, allElem, corner, en2, nr, comm;
+};
+
+DomSizes sizes_of(int nx, int numReg, long comm_doubles);
+size_t align256(size_t b);
+// device bytes of one domain (all of its arrays at 256-byte alignment)
+size_t domain_bytes(const DomSizes &s, bool mixed);
+// receive-buffer doubles of a rank in a tp^3 decomposition (0 for tp = 1)
+long comm_buffer_doubles(int nx, int tp);
+
+// Hands out consecutive 256-byte-aligned pieces of one allocation.
+struct Carver {
+    char *base;
+    size_t off = 0;
+    template <typename T> T *take(size_t count)
+    {
+        T *p = reinterpret_cast<T *>(base + off);
+        off += align256(sizeof(T) * count);
+        return p;
+    }
+};
+
+// Carve every array of host domain `h` from `cv`, initialise and upload it
+// on `st`, and fill the device record *D (and *c32 when mixed).  `tc` is
+// the TimeCtl slot of the domain's job.  Synchronises `st` before
+// returning, so `h` may be released afterwards.
+int upload_domain(const HostDomain &h, int tc, long comm_doubles, bool mixed, Carver &cv,
+                  cudaStream_t st, DomDev *D, CornerF32 *c32);
+
+// The time state of a job before its first cycle (lulesh.cu:1120-1132).
+TimeCtl initial_timectl(double deltatime, int its_cap);
+
+}  // namespace lulesh

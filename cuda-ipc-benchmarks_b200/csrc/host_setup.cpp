@@ -1,6 +1,7 @@
 // host_setup.cpp -- host-side construction of LULESH domains (see header).
 #include "host_setup.hpp"
 
+#include <algorithm>
 #include <climits>
 #include <cmath>
 
@@ -199,6 +200,31 @@ static void build_regions(HostDomain &d, int nr, int balance)
         int r = d.regSorted[d.regNumList[i] - 1];
         d.regElemlist[d.regCSR[r]] = i;
         d.regCSR[r]++;
+    }
+
+    // EOS work order.  Each element's rep count is that of its region
+    // (regReps is sorted with the regions); the EOS of an element depends
+    // only on that element, so the order elements are visited in is free.
+    // Grouping by rep count keeps a warp's trip count uniform, like the
+    // reference's per-region order, while the classes (at most three) are
+    // far denser than single regions, so a warp's loads share cache lines.
+    std::vector<int> rep_of(E);
+    std::vector<int> distinct;
+    for (int i = 0; i < E; ++i) {
+        rep_of[i] = d.regReps[d.regSorted[d.regNumList[i] - 1]];
+        bool seen = false;
+        for (int v : distinct) seen = seen || (v == rep_of[i]);
+        if (!seen) distinct.push_back(rep_of[i]);
+    }
+    std::sort(distinct.begin(), distinct.end(), [](int a, int b) { return a > b; });
+    d.eosOrder.clear();
+    d.eosOrder.reserve(E);
+    d.eosNumClass = (int)distinct.size();
+    for (int c = 0; c < d.eosNumClass; ++c) {
+        for (int i = 0; i < E; ++i)
+            if (rep_of[i] == distinct[c]) d.eosOrder.push_back(i);
+        d.eosClassEnd[c] = (int)d.eosOrder.size();
+        d.eosClassRep[c] = distinct[c];
     }
 }
 

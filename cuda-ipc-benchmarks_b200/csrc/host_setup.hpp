@@ -37,6 +37,13 @@ struct HostDomain {
     std::vector<int> nodeElemCount, nodeElemStart, nodeElemCornerList;
     std::vector<int> symmX, symmY, symmZ, matElemlist;
     std::vector<int> regElemSize, regCSR, regReps, regNumList, regElemlist, regSorted;
+    // EOS work order: elements grouped by their rep count (heaviest class
+    // first), ascending element index inside a class; class c covers
+    // positions [eosClassEnd[c-1], eosClassEnd[c]) and runs eosClassRep[c]
+    std::vector<int> eosOrder;
+    int eosNumClass = 0;
+    int eosClassEnd[kMaxRepClasses] = {0};
+    int eosClassRep[kMaxRepClasses] = {0};
     std::vector<double> x, y, z, volo, elemMass, nodalMass, e;
     double einit = 0.0;
     double deltatime = 0.0;  // initial dt of this domain, lulesh.cu:1205

@@ -126,11 +126,34 @@ __device__ __forceinline__ void elem_nodes(const DomDev &D, int el, int n[8])
     n[7] = n0 + en * en + en;
 }
 
+// Start the velocity gathers of an element's eight nodes early, so that
+// the loads issued after the coordinate arithmetic hit in cache.
+__device__ __forceinline__ void prefetch_velocities(const DomDev &D, const int n[8])
+{
+#if LULESH_VEL_PREFETCH == 1 || LULESH_VEL_PREFETCH == 2
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+#if LULESH_VEL_PREFETCH == 1
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(D.xd + n[i]));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(D.yd + n[i]));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(D.zd + n[i]));
+#else
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(D.xd + n[i]));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(D.yd + n[i]));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(D.zd + n[i]));
+#endif
+    }
+#else
+    (void)D;
+    (void)n;
+#endif
+}
+
 // ---------------------------------------------------------------------------
 // force: CalcVolumeForceForElems_kernel, lulesh.cu:2080-2259
 
 template <bool HG>
-__global__ void __launch_bounds__(kElemBlock) k_force(SetArgs a, Params P)
+__global__ void __launch_bounds__(kElemBlock, kForceMinBlocks) k_force(SetArgs a, Params P)
 {
     const int2 blk = a.blocks[blockIdx.x];
     const DomDev &D = a.doms[blk.x];
@@ -154,6 +177,19 @@ __global__ void __launch_bounds__(kElemBlock) k_force(SetArgs a, Params P)
 
     int n[8];
     elem_nodes(D, elem, n);
+#if LULESH_VEL_PREFETCH == 3
+    double xdn[8], ydn[8], zdn[8];
+    if (HG) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            xdn[i] = D.xd[n[i]];
+            ydn[i] = D.yd[n[i]];
+            zdn[i] = D.zd[n[i]];
+        }
+    }
+#else
+    if (HG) prefetch_velocities(D, n);
+#endif
     const double volinv = 1.0 / det;
 #pragma unroll
     for (int i = 0; i < 8; ++i) xn[i] = D.x[n[i]];
@@ -181,6 +217,11 @@ __global__ void __launch_bounds__(kElemBlock) k_force(SetArgs a, Params P)
         hgfz[i] = -(sigxx * B[2][i]);
     }
     if (HG) {
+#if LULESH_VEL_PREFETCH == 3
+        fb_hourglass_component(xdn, hourgam, coefficient, hgfx);
+        fb_hourglass_component(ydn, hourgam, coefficient, hgfy);
+        fb_hourglass_component(zdn, hourgam, coefficient, hgfz);
+#else
         double vel[8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) vel[i] = D.xd[n[i]];
@@ -191,6 +232,7 @@ __global__ void __launch_bounds__(kElemBlock) k_force(SetArgs a, Params P)
 #pragma unroll
         for (int i = 0; i < 8; ++i) vel[i] = D.zd[n[i]];
         fb_hourglass_component(vel, hourgam, coefficient, hgfz);
+#endif
     }
     const int Ep = D.Ep;
 #pragma unroll
@@ -343,7 +385,7 @@ void launch_nodal_update(const SetArgs &a, int nblocks, Params P, cudaStream_t s
 // ---------------------------------------------------------------------------
 // kinematics: CalcKinematicsAndMonotonicQGradient_kernel, lulesh.cu:3343-3507
 
-__global__ void __launch_bounds__(kElemBlock) k_kinematics(SetArgs a, Params P)
+__global__ void __launch_bounds__(kElemBlock, kKinMinBlocks) k_kinematics(SetArgs a, Params P)
 {
     const int2 blk = a.blocks[blockIdx.x];
     const DomDev &D = a.doms[blk.x];
@@ -358,6 +400,16 @@ __global__ void __launch_bounds__(kElemBlock) k_kinematics(SetArgs a, Params P)
     double Dv[3];
     int nodes[8];
     elem_nodes(D, k, nodes);
+#if LULESH_VEL_PREFETCH == 3
+#pragma unroll
+    for (int l = 0; l < 8; ++l) {
+        xd_local[l] = D.xd[nodes[l]];
+        yd_local[l] = D.yd[nodes[l]];
+        zd_local[l] = D.zd[nodes[l]];
+    }
+#else
+    prefetch_velocities(D, nodes);
+#endif
 #pragma unroll
     for (int l = 0; l < 8; ++l) x_local[l] = D.x[nodes[l]];
 #pragma unroll
@@ -371,6 +423,7 @@ __global__ void __launch_bounds__(kElemBlock) k_kinematics(SetArgs a, Params P)
     D.delv[k] = relativeVolume - D.v[k];
     D.arealg[k] = elem_characteristic_length(x_local, y_local, z_local, volume);
 
+#if LULESH_VEL_PREFETCH != 3
 #pragma unroll
     for (int l = 0; l < 8; ++l) {
         const int g = nodes[l];
@@ -378,6 +431,7 @@ __global__ void __launch_bounds__(kElemBlock) k_kinematics(SetArgs a, Params P)
         yd_local[l] = D.yd[g];
         zd_local[l] = D.zd[g];
     }
+#endif
     const double dt2 = 0.5 * T.deltatime;
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
@@ -419,6 +473,53 @@ void launch_kinematics(const SetArgs &a, int nblocks, Params P, cudaStream_t s)
 
 // ---------------------------------------------------------------------------
 // eos: monotonic Q region + EOS + volume update + dt constraints
+
+// Boundary-condition mask and the six face-neighbour indices of element z,
+// computed from its position: the values SetupConnectivityBC stores in
+// elemBC and lxim..lzetap (lulesh.cu:537-686).  Interior neighbours are the
+// adjacent elements; a face on the mesh boundary is a symmetry plane at the
+// minimum and a free surface at the maximum; a face against another
+// subdomain is a comm face whose neighbour is a ghost element (ghost face
+// offsets in the order planeMin, planeMax, rowMin, rowMax, colMin, colMax).
+// Indices the limiter does not read for a given mask are left as is.
+__device__ __forceinline__ void elem_face_links(const DomDev &D, int z, int &bc, int &xm,
+                                                int &xp, int &em, int &ep, int &zm, int &zp)
+{
+    const int nx = D.nx, nn = nx * nx;
+    const int ix = z % nx, t = z / nx, iy = t % nx, iz = t / nx;
+    bc = 0;
+    xm = z - 1;
+    xp = z + 1;
+    em = z - nx;
+    ep = z + nx;
+    zm = z - nn;
+    zp = z + nn;
+    const int last = D.tp - 1;
+    if (iz == 0) {
+        if (D.plane == 0) bc |= ZETA_M_SYMM;
+        else { bc |= ZETA_M_COMM; zm = D.ghost[0] + iy * nx + ix; }
+    }
+    if (iz == nx - 1) {
+        if (D.plane == last) bc |= ZETA_P_FREE;
+        else { bc |= ZETA_P_COMM; zp = D.ghost[1] + iy * nx + ix; }
+    }
+    if (iy == 0) {
+        if (D.row == 0) bc |= ETA_M_SYMM;
+        else { bc |= ETA_M_COMM; em = D.ghost[2] + iz * nx + ix; }
+    }
+    if (iy == nx - 1) {
+        if (D.row == last) bc |= ETA_P_FREE;
+        else { bc |= ETA_P_COMM; ep = D.ghost[3] + iz * nx + ix; }
+    }
+    if (ix == 0) {
+        if (D.col == 0) bc |= XI_M_SYMM;
+        else { bc |= XI_M_COMM; xm = D.ghost[4] + iz * nx + iy; }
+    }
+    if (ix == nx - 1) {
+        if (D.col == last) bc |= XI_P_FREE;
+        else { bc |= XI_P_COMM; xp = D.ghost[5] + iz * nx + iy; }
+    }
+}
 
 // one direction of the monotonic limiter, lulesh.cu:3595-3624
 __device__ __forceinline__ double mono_limiter(const double *delv, int i, int bc, int mmask,
@@ -535,7 +636,7 @@ __device__ __forceinline__ double warp_min(double v)
     return v;
 }
 
-__global__ void __launch_bounds__(kElemBlock) k_eos(SetArgs a, Params P)
+__global__ void __launch_bounds__(kElemBlock, kEosMinBlocks) k_eos(SetArgs a, Params P)
 {
     const int2 blk = a.blocks[blockIdx.x];
     const DomDev &D = a.doms[blk.x];
@@ -544,22 +645,31 @@ __global__ void __launch_bounds__(kElemBlock) k_eos(SetArgs a, Params P)
     const int i = blk.y + threadIdx.x;
     double dtc = 1.0e+20, dth = 1.0e+20;
     if (i < D.numElem) {
-        const int zidx = D.regElemlist[i];
+        // The element of this slot and its rep count.  The reference visits
+        // regElemlist and finds the rep by region (giveMyRegion,
+        // lulesh.cu:3976-3984); here slots are grouped by rep class
+        // (HostDomain::eosOrder), which keeps the trip count uniform per warp
+        // with denser loads (measured 98 us vs 99 us regElemlist order and
+        // 108 us natural order at -s 100).
+        const int zidx = D.eosOrder[i];
+        int cls = 0;
+        while (cls < D.eosNumClass - 1 && i >= D.eosClassEnd[cls]) ++cls;
+        const int rep = D.eosClassRep[cls];
 
         // ---- CalcMonotonicQRegionForElems_kernel, lulesh.cu:3586-3724
         const double ptiny = 1.e-36;
-        const int bcMask = D.elemBC[zidx];
+        int bcMask, lxm, lxp, lem, lep, lzm, lzp;
+        elem_face_links(D, zidx, bcMask, lxm, lxp, lem, lep, lzm, lzp);
         const double mult = P.monoq_limiter_mult, maxs = P.monoq_max_slope;
         const double phixi =
             mono_limiter(D.delv_xi, zidx, bcMask, XI_M, XI_M_SYMM, XI_M_FREE, XI_P, XI_P_SYMM,
-                         XI_P_FREE, D.lxim[zidx], D.lxip[zidx], mult, maxs, ptiny);
+                         XI_P_FREE, lxm, lxp, mult, maxs, ptiny);
         const double phieta =
             mono_limiter(D.delv_eta, zidx, bcMask, ETA_M, ETA_M_SYMM, ETA_M_FREE, ETA_P,
-                         ETA_P_SYMM, ETA_P_FREE, D.letam[zidx], D.letap[zidx], mult, maxs, ptiny);
+                         ETA_P_SYMM, ETA_P_FREE, lem, lep, mult, maxs, ptiny);
         const double phizeta =
             mono_limiter(D.delv_zeta, zidx, bcMask, ZETA_M, ZETA_M_SYMM, ZETA_M_FREE, ZETA_P,
-                         ZETA_P_SYMM, ZETA_P_FREE, D.lzetam[zidx], D.lzetap[zidx], mult, maxs,
-                         ptiny);
+                         ZETA_P_SYMM, ZETA_P_FREE, lzm, lzp, mult, maxs, ptiny);
         const double vdov_z = D.vdov[zidx];
         const double vnew_z = D.vnew[zidx];
         double qlin, qquad;
@@ -606,15 +716,6 @@ __global__ void __launch_bounds__(kElemBlock) k_eos(SetArgs a, Params P)
             if (vc > eosvmax) vc = eosvmax;
         }
         if (vc <= 0.) atomicMin(&T.bad_vol, zidx);
-
-        // giveMyRegion (lulesh.cu:3976-3984): regCSR holds region ends
-        int region = D.numReg - 1;
-        for (int r = 0; r < D.numReg - 1; ++r)
-            if (i < D.regCSR[r]) {
-                region = r;
-                break;
-            }
-        const int rep = D.regReps[region];
 
         double e_old, delvc, p_old, q_old, compression, compHalfStep, qq_old, ql_old, work;
         double p_new = 0., e_new = 0., q_new = 0., bvc = 0., pbvc = 0.;

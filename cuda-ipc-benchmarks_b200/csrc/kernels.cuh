@@ -10,6 +10,32 @@ namespace lulesh {
 constexpr int kElemBlock = 128;  // threads per block, element kernels
 constexpr int kNodeBlock = 128;  // threads per block, node kernels
 
+// Resident blocks per SM asked of the compiler (the register budget of the
+// element kernels), chosen by measurement on B200 at -s 100: kinematics 3
+// (<= 170 registers, 118 -> 92 us), EOS 8 (64 registers, 134 -> 98 us).
+#ifndef LULESH_FORCE_MINB
+#define LULESH_FORCE_MINB 1
+#endif
+#ifndef LULESH_FORCECP_MINB
+#define LULESH_FORCECP_MINB 1
+#endif
+#ifndef LULESH_KIN_MINB
+#define LULESH_KIN_MINB 3
+#endif
+#ifndef LULESH_EOS_MINB
+#define LULESH_EOS_MINB 8
+#endif
+// Velocity gathers of the force and kinematics kernels: 0 where the
+// arithmetic first needs them, 1 prefetched into L1 at kernel start,
+// 2 prefetched into L2 at kernel start, 3 loaded into registers at start.
+#ifndef LULESH_VEL_PREFETCH
+#define LULESH_VEL_PREFETCH 0
+#endif
+constexpr int kForceCpMinBlocks = LULESH_FORCECP_MINB;
+constexpr int kForceMinBlocks = LULESH_FORCE_MINB;
+constexpr int kKinMinBlocks = LULESH_KIN_MINB;
+constexpr int kEosMinBlocks = LULESH_EOS_MINB;
+
 // A kernel launch over all domains of a set: block b works on domain
 // blocks[b].x starting at item blocks[b].y (element, node or region slot).
 struct SetArgs {
@@ -21,6 +47,14 @@ struct SetArgs {
 
 void launch_time_increment(TimeCtl *tcs, int ntc, Params P, cudaStream_t s);
 void launch_force(const SetArgs &a, int nblocks, Params P, cudaStream_t s);
+// corner-parallel force kernel: 8 threads per element, kCpElemsPerBlock
+// elements per block (blocks[] built with that step)
+constexpr int kCpElemsPerBlock = 32;
+void launch_force_cp(const SetArgs &a, int nblocks, Params P, cudaStream_t s);
+// 0: element per thread (k_force), 1: corner-parallel (k_force_cp)
+#ifndef LULESH_FORCE_CP
+#define LULESH_FORCE_CP 0
+#endif
 void launch_nodal(const SetArgs &a, int nblocks, Params P, cudaStream_t s);
 // staged comm path: own-corner partial sums, then the update from fx/fy/fz
 void launch_nodal_gather_local(const SetArgs &a, int nblocks, cudaStream_t s);

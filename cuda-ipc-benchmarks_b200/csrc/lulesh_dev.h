@@ -21,6 +21,10 @@ enum : int {
     ZETA_P = 0x38000, ZETA_P_SYMM = 0x08000, ZETA_P_FREE = 0x10000, ZETA_P_COMM = 0x20000
 };
 
+// Distinct EOS rep counts a domain can have: 1, 1+cost, 10*(1+cost)
+// (CreateRegionIndexSets, lulesh.cu:1364-1374).
+constexpr int kMaxRepClasses = 4;
+
 // Material / control parameters of NewDomain, lulesh.cu:1125-1158.
 struct Params {
     double dtfixed, deltatimemultlb, deltatimemultub, stoptime, dtmax;
@@ -71,6 +75,11 @@ struct DomDev {
     int *symmX, *symmY, *symmZ, *matElemlist;
     int *regCSR, *regReps, *regNumList, *regElemlist, *regSorted;
     int numSymmX, numSymmY, numSymmZ;
+    // EOS work order (see HostDomain::eosOrder)
+    int *eosOrder;
+    int eosNumClass;
+    int eosClassEnd[kMaxRepClasses];
+    int eosClassRep[kMaxRepClasses];
     // comm message buffers (staged exchange): receive buffer of this rank
     double *commRecv;
     long commRecvLen;

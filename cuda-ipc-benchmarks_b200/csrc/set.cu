@@ -6,6 +6,7 @@
 #include <mutex>
 #include <string>
 
+#include "domain_dev.hpp"
 #include "set.hpp"
 
 namespace lulesh {
@@ -29,88 +30,6 @@ int cuda_status(cudaError_t e, const char *what)
         if (_st != LULESH_OK) return _st;                       \
     } while (0)
 
-// ---- arena sizing ---------------------------------------------------------
-
-struct DomSizes {
-    size_t E, N, Ep, allElem, corner, en2, nr, comm;
-};
-
-static DomSizes sizes_of(int nx, int numReg, long comm_doubles)
-{
-    DomSizes s;
-    s.E = (size_t)nx * nx * nx;
-    s.N = (size_t)(nx + 1) * (nx + 1) * (nx + 1);
-    s.Ep = ((s.E + 31) / 32) * 32;
-    s.allElem = s.E + 6 * (size_t)nx * nx;
-    s.corner = 8 * s.E;
-    s.en2 = (size_t)(nx + 1) * (nx + 1);
-    s.nr = (size_t)numReg;
-    s.comm = (size_t)comm_doubles;
-    return s;
-}
-
-static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
-
-static size_t domain_bytes(const DomSizes &s, bool mixed)
-{
-    size_t b = 0;
-    b += 16 * align256(8 * s.E);        // element doubles incl. vnew, delx_*
-    b += 3 * align256(8 * s.allElem);   // delv_* with ghost faces
-    b += 13 * align256(8 * s.N);        // node doubles
-    b += 3 * align256(8 * 8 * s.Ep);    // corner forces
-    b += align256(4 * 8 * s.Ep);        // nodelist
-    b += 10 * align256(4 * s.E);        // l*, elemBC, matElemlist, regNumList, regElemlist
-    b += 2 * align256(4 * s.N);         // nodeElemCount/Start
-    b += align256(4 * s.corner);        // nodeElemCornerList
-    b += 3 * align256(4 * s.en2);       // symm*
-    b += 3 * align256(4 * s.nr);        // regCSR, regReps, regSorted
-    if (s.comm) b += align256(8 * s.comm);
-    if (mixed) b += 3 * align256(4 * 8 * s.Ep);
-    return b;
-}
-
-// receive-buffer capacity of SetupCommBuffers, lulesh.cu:457-510, for a
-// domain with all 26 neighbours (the worst case every rank is sized for)
-static long comm_buffer_doubles(int nx, int tp)
-{
-    if (tp <= 1) return 0;
-    const long pad = 16;  // CACHE_COHERENCE_PAD_REAL for doubles
-    long maxEdge = nx + 1;
-    long maxPlane = ((maxEdge * maxEdge + pad - 1) / pad) * pad;
-    maxEdge = ((maxEdge + pad - 1) / pad) * pad;
-    (void)maxEdge;
-    return 6 * maxPlane * 6 + 12 * maxPlane * 6 + 8 * pad;
-}
-
-// ---- device helpers ----------------------------------------------------------
-
-struct Carver {
-    char *base;
-    size_t off = 0;
-    template <typename T> T *take(size_t count)
-    {
-        T *p = reinterpret_cast<T *>(base + off);
-        off += align256(sizeof(T) * count);
-        return p;
-    }
-};
-
-template <typename T>
-static int upload(T *dst, const std::vector<T> &src, cudaStream_t s)
-{
-    if (src.empty()) return LULESH_OK;
-    return cuda_status(cudaMemcpyAsync(dst, src.data(), sizeof(T) * src.size(),
-                                       cudaMemcpyHostToDevice, s),
-                       "upload");
-}
-
-static unsigned long long dbl_bits(double v)
-{
-    unsigned long long u;
-    std::memcpy(&u, &v, sizeof u);
-    return u;
-}
-
 // ---- creation -------------------------------------------------------------
 
 static int validate_job(const lulesh_job &j)
@@ -125,10 +44,11 @@ static int validate_job(const lulesh_job &j)
 
 static int build_tables(lulesh_set *s)
 {
-    std::vector<int2> eb, nb, gb;
+    std::vector<int2> eb, nb, gb, cb;
     for (int d = 0; d < s->ndom; ++d) {
         const DomDev &D = s->hdoms[d];
         for (int i = 0; i < D.numElem; i += kElemBlock) eb.push_back(make_int2(d, i));
+        for (int i = 0; i < D.numElem; i += kCpElemsPerBlock) cb.push_back(make_int2(d, i));
         for (int i = 0; i < D.numNode; i += kNodeBlock) nb.push_back(make_int2(d, i));
         if (D.tp > 1)
             for (int f = 0; f < 6; ++f)
@@ -139,12 +59,16 @@ static int build_tables(lulesh_set *s)
     s->n_elem_blocks = (int)eb.size();
     s->n_node_blocks = (int)nb.size();
     s->n_ghost_blocks = (int)gb.size();
-    size_t bytes = sizeof(int2) * (eb.size() + nb.size() + gb.size() + 1);
+    s->n_cp_blocks = (int)cb.size();
+    size_t bytes = sizeof(int2) * (eb.size() + nb.size() + gb.size() + cb.size() + 1);
     int2 *t = nullptr;
     LCHECK(cudaMalloc(&t, bytes));
     s->elem_blocks = t;
     s->node_blocks = t + eb.size();
     s->ghost_blocks = t + eb.size() + nb.size();
+    s->cp_blocks = t + eb.size() + nb.size() + gb.size();
+    LCHECK(cudaMemcpyAsync(s->cp_blocks, cb.data(), sizeof(int2) * cb.size(),
+                           cudaMemcpyHostToDevice, s->stream));
     LCHECK(cudaMemcpyAsync(s->elem_blocks, eb.data(), sizeof(int2) * eb.size(),
                            cudaMemcpyHostToDevice, s->stream));
     LCHECK(cudaMemcpyAsync(s->node_blocks, nb.data(), sizeof(int2) * nb.size(),
@@ -199,105 +123,9 @@ static int create_common(lulesh_set *s, const std::vector<DomPlace> &place, int 
         HostDomain h;
         build_domain(h, j.nx, pl.tp, pl.col, pl.row, pl.plane, pl.rank, j.numReg, j.balance,
                      j.cost, /*global_mass=*/pl.tp > 1);
-        DomSizes z = sizes_of(j.nx, j.numReg, commd[d]);
         DomDev D{};
-        D.nx = j.nx;
-        D.en = j.nx + 1;
-        D.numElem = h.numElem;
-        D.numNode = h.numNode;
-        D.Ep = h.Ep;
-        D.allElem = h.allElem;
-        D.col = pl.col;
-        D.row = pl.row;
-        D.plane = pl.plane;
-        D.tp = pl.tp;
-        D.tc = pl.job;
-        D.numReg = j.numReg;
-        D.numSymmX = h.numSymmX;
-        D.numSymmY = h.numSymmY;
-        D.numSymmZ = h.numSymmZ;
-        for (int f = 0; f < 6; ++f) D.ghost[f] = h.ghost[f];
-        for (int k = 0; k < 27; ++k) D.nbr[k] = -1;
-        // element doubles
-        D.e = cv.take<double>(z.E); D.p = cv.take<double>(z.E); D.q = cv.take<double>(z.E);
-        D.ql = cv.take<double>(z.E); D.qq = cv.take<double>(z.E); D.v = cv.take<double>(z.E);
-        D.volo = cv.take<double>(z.E); D.delv = cv.take<double>(z.E);
-        D.vdov = cv.take<double>(z.E); D.arealg = cv.take<double>(z.E);
-        D.ss = cv.take<double>(z.E); D.elemMass = cv.take<double>(z.E);
-        D.vnew = cv.take<double>(z.E); D.delx_xi = cv.take<double>(z.E);
-        D.delx_eta = cv.take<double>(z.E); D.delx_zeta = cv.take<double>(z.E);
-        D.delv_xi = cv.take<double>(z.allElem); D.delv_eta = cv.take<double>(z.allElem);
-        D.delv_zeta = cv.take<double>(z.allElem);
-        // node doubles
-        D.x = cv.take<double>(z.N); D.y = cv.take<double>(z.N); D.z = cv.take<double>(z.N);
-        D.xd = cv.take<double>(z.N); D.yd = cv.take<double>(z.N); D.zd = cv.take<double>(z.N);
-        D.xdd = cv.take<double>(z.N); D.ydd = cv.take<double>(z.N); D.zdd = cv.take<double>(z.N);
-        D.fx = cv.take<double>(z.N); D.fy = cv.take<double>(z.N); D.fz = cv.take<double>(z.N);
-        D.nodalMass = cv.take<double>(z.N);
-        D.fx_elem = cv.take<double>(8 * z.Ep); D.fy_elem = cv.take<double>(8 * z.Ep);
-        D.fz_elem = cv.take<double>(8 * z.Ep);
-        // ints
-        D.nodelist = cv.take<int>(8 * z.Ep);
-        D.lxim = cv.take<int>(z.E); D.lxip = cv.take<int>(z.E); D.letam = cv.take<int>(z.E);
-        D.letap = cv.take<int>(z.E); D.lzetam = cv.take<int>(z.E); D.lzetap = cv.take<int>(z.E);
-        D.elemBC = cv.take<int>(z.E); D.matElemlist = cv.take<int>(z.E);
-        D.regNumList = cv.take<int>(z.E); D.regElemlist = cv.take<int>(z.E);
-        D.nodeElemCount = cv.take<int>(z.N); D.nodeElemStart = cv.take<int>(z.N);
-        D.nodeElemCornerList = cv.take<int>(z.corner);
-        D.symmX = cv.take<int>(z.en2); D.symmY = cv.take<int>(z.en2); D.symmZ = cv.take<int>(z.en2);
-        D.regCSR = cv.take<int>(z.nr); D.regReps = cv.take<int>(z.nr); D.regSorted = cv.take<int>(z.nr);
-        if (z.comm) {
-            D.commRecv = cv.take<double>(z.comm);
-            D.commRecvLen = (long)z.comm;
-        }
-        if (mixed) {
-            CornerF32 &c = hc32[d];
-            c.fx = cv.take<float>(8 * z.Ep); c.fy = cv.take<float>(8 * z.Ep);
-            c.fz = cv.take<float>(8 * z.Ep);
-        }
-
-        // upload (InitializeFields: zeros except v = 1, lulesh.cu:432-451)
-        cudaStream_t st = s->stream;
-        const size_t E = z.E, N = z.N;
-        double *edbl[16] = {D.e, D.p, D.q, D.ql, D.qq, D.v, D.volo, D.delv, D.vdov,
-                            D.arealg, D.ss, D.elemMass, D.vnew, D.delx_xi, D.delx_eta,
-                            D.delx_zeta};
-        for (double *p : edbl) LCHECK(cudaMemsetAsync(p, 0, 8 * E, st));
-        double *ndbl[13] = {D.x, D.y, D.z, D.xd, D.yd, D.zd, D.xdd, D.ydd, D.zdd,
-                            D.fx, D.fy, D.fz, D.nodalMass};
-        for (double *p : ndbl) LCHECK(cudaMemsetAsync(p, 0, 8 * N, st));
-        LCHECK(cudaMemsetAsync(D.delv_xi, 0, 8 * z.allElem, st));
-        LCHECK(cudaMemsetAsync(D.delv_eta, 0, 8 * z.allElem, st));
-        LCHECK(cudaMemsetAsync(D.delv_zeta, 0, 8 * z.allElem, st));
-        LCHECK(cudaMemsetAsync(D.fx_elem, 0, 8 * 8 * z.Ep, st));
-        LCHECK(cudaMemsetAsync(D.fy_elem, 0, 8 * 8 * z.Ep, st));
-        LCHECK(cudaMemsetAsync(D.fz_elem, 0, 8 * 8 * z.Ep, st));
-        if (z.comm) LCHECK(cudaMemsetAsync(D.commRecv, 0, 8 * z.comm, st));
-        std::vector<double> ones(E, 1.0);
-        int st_up;
-        if ((st_up = upload(D.v, ones, st)) != LULESH_OK) return st_up;
-        if ((st_up = upload(D.e, h.e, st)) != LULESH_OK) return st_up;
-        if ((st_up = upload(D.volo, h.volo, st)) != LULESH_OK) return st_up;
-        if ((st_up = upload(D.elemMass, h.elemMass, st)) != LULESH_OK) return st_up;
-        if ((st_up = upload(D.x, h.x, st)) != LULESH_OK) return st_up;
-        if ((st_up = upload(D.y, h.y, st)) != LULESH_OK) return st_up;
-        if ((st_up = upload(D.z, h.z, st)) != LULESH_OK) return st_up;
-        if ((st_up = upload(D.nodalMass, h.nodalMass, st)) != LULESH_OK) return st_up;
-        if ((st_up = upload(D.nodelist, h.nodelist, st)) != LULESH_OK) return st_up;
-        const std::vector<int> *iv[] = {&h.lxim, &h.lxip, &h.letam, &h.letap, &h.lzetam,
-                                        &h.lzetap, &h.elemBC, &h.matElemlist, &h.regNumList,
-                                        &h.regElemlist, &h.nodeElemCount, &h.nodeElemStart,
-                                        &h.nodeElemCornerList, &h.symmX, &h.symmY, &h.symmZ,
-                                        &h.regCSR, &h.regReps, &h.regSorted};
-        int *ip[] = {D.lxim, D.lxip, D.letam, D.letap, D.lzetam, D.lzetap, D.elemBC,
-                     D.matElemlist, D.regNumList, D.regElemlist, D.nodeElemCount,
-                     D.nodeElemStart, D.nodeElemCornerList, D.symmX, D.symmY, D.symmZ,
-                     D.regCSR, D.regReps, D.regSorted};
-        for (size_t k = 0; k < sizeof(ip) / sizeof(ip[0]); ++k)
-            if ((st_up = upload(ip[k], *iv[k], st)) != LULESH_OK) return st_up;
-        // host vectors must outlive the async copies
-        LCHECK(cudaStreamSynchronize(st));
-
+        int su = upload_domain(h, pl.job, commd[d], mixed, cv, s->stream, &D, &hc32[d]);
+        if (su != LULESH_OK) return su;
         s->hdoms[d] = D;
         s->dom_rank[d] = pl.rank;
         s->dom_job[d] = pl.job;
@@ -331,20 +159,7 @@ static int create_common(lulesh_set *s, const std::vector<DomPlace> &place, int 
 
     // time control blocks
     std::vector<TimeCtl> tc(s->njobs);
-    for (int j = 0; j < s->njobs; ++j) {
-        TimeCtl &T = tc[j];
-        std::memset(&T, 0, sizeof T);
-        T.time = 0.0;
-        T.deltatime = job_dt[j];
-        T.dtcourant = 1.0e+20;
-        T.dthydro = 1.0e+20;
-        T.min_courant = dbl_bits(1.0e+20);
-        T.min_hydro = dbl_bits(1.0e+20);
-        T.cycle = 0;
-        T.its_cap = s->jobs[j].its;
-        T.bad_vol = INT_MAX;
-        T.bad_q = INT_MAX;
-    }
+    for (int j = 0; j < s->njobs; ++j) tc[j] = initial_timectl(job_dt[j], s->jobs[j].its);
     LCHECK(cudaMalloc(&s->dtc, sizeof(TimeCtl) * s->njobs));
     LCHECK(cudaMallocHost(&s->htc_pinned, sizeof(TimeCtl) * s->njobs));
     LCHECK(cudaMemcpyAsync(s->dtc, tc.data(), sizeof(TimeCtl) * s->njobs,
@@ -353,6 +168,15 @@ static int create_common(lulesh_set *s, const std::vector<DomPlace> &place, int 
     if (st != LULESH_OK) return st;
     LCHECK(cudaStreamSynchronize(s->stream));
     return LULESH_OK;
+}
+
+void launch_force_fp64(lulesh_set *s, cudaStream_t st)
+{
+#if LULESH_FORCE_CP
+    launch_force_cp(s->args(s->cp_blocks), s->n_cp_blocks, s->P, st);
+#else
+    launch_force(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st);
+#endif
 }
 
 int enqueue_cycle(lulesh_set *s)
@@ -364,7 +188,7 @@ int enqueue_cycle(lulesh_set *s)
     if (mixed)
         launch_force_mixed(s->args(s->elem_blocks), s->n_elem_blocks, s->P, s->dcorner32, st);
     else
-        launch_force(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st);
+        launch_force_fp64(s, st);
     if (mixed)
         launch_nodal_mixed(s->args(s->node_blocks), s->n_node_blocks, s->P, s->dcorner32, st);
     else
@@ -402,8 +226,34 @@ static int ensure_graph(lulesh_set *s)
     return LULESH_OK;
 }
 
+// graph of graph_cycles consecutive cycles (one launch for many cycles)
+static int ensure_graph_k(lulesh_set *s)
+{
+    if (s->graph_k_ready || s->graph_cycles <= 1) return LULESH_OK;
+    int st = ensure_graph(s);  // prepares comm tables when staged
+    if (st != LULESH_OK) return st;
+    LCHECK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    for (int c = 0; c < s->graph_cycles && st == LULESH_OK; ++c) st = enqueue_cycle(s);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+    if (st != LULESH_OK) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+    }
+    LCHECK(e);
+    s->graph_k = g;
+    LCHECK(cudaGraphInstantiate(&s->exec_k, g, 0));
+    s->graph_k_ready = true;
+    return LULESH_OK;
+}
+
 static void drop_graph(lulesh_set *s)
 {
+    if (s->exec_k) cudaGraphExecDestroy(s->exec_k);
+    if (s->graph_k) cudaGraphDestroy(s->graph_k);
+    s->exec_k = nullptr;
+    s->graph_k = nullptr;
+    s->graph_k_ready = false;
     if (s->exec) cudaGraphExecDestroy(s->exec);
     if (s->graph) cudaGraphDestroy(s->graph);
     s->exec = nullptr;
@@ -636,7 +486,27 @@ int lulesh_step(lulesh_set *s, int ncycles)
     if (!s || ncycles < 0) return LULESH_INVALID_ARG;
     int st = ensure_graph(s);
     if (st != LULESH_OK) return st;
+    if (s->graph_cycles > 1 && ncycles >= s->graph_cycles) {
+        if ((st = ensure_graph_k(s)) != LULESH_OK) return st;
+        for (; ncycles >= s->graph_cycles; ncycles -= s->graph_cycles)
+            LCHECK(cudaGraphLaunch(s->exec_k, s->stream));
+    }
     for (int i = 0; i < ncycles; ++i) LCHECK(cudaGraphLaunch(s->exec, s->stream));
+    return LULESH_OK;
+}
+
+int lulesh_set_graph_cycles(lulesh_set *s, int k)
+{
+    if (!s || k < 1 || k > 100000) return LULESH_INVALID_ARG;
+    if (k != s->graph_cycles) {
+        LCHECK(cudaStreamSynchronize(s->stream));
+        if (s->exec_k) cudaGraphExecDestroy(s->exec_k);
+        if (s->graph_k) cudaGraphDestroy(s->graph_k);
+        s->exec_k = nullptr;
+        s->graph_k = nullptr;
+        s->graph_k_ready = false;
+        s->graph_cycles = k;
+    }
     return LULESH_OK;
 }
 
@@ -725,7 +595,7 @@ int lulesh_profile_phases(lulesh_set *s, int ncycles, double *ms_out, int *nphas
         if (mixed)
             launch_force_mixed(s->args(s->elem_blocks), s->n_elem_blocks, s->P, s->dcorner32, st);
         else
-            launch_force(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st);
+            launch_force_fp64(s, st);
         LCHECK(cudaEventRecord(ev[2], st));
         if (mixed)
             launch_nodal_mixed(s->args(s->node_blocks), s->n_node_blocks, s->P, s->dcorner32, st);

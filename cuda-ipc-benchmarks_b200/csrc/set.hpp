@@ -33,7 +33,8 @@ struct lulesh_set {
     lulesh::TimeCtl *dtc = nullptr;
     lulesh::TimeCtl *htc_pinned = nullptr;  // pinned mirror for readback
     int2 *elem_blocks = nullptr, *node_blocks = nullptr, *ghost_blocks = nullptr;
-    int n_elem_blocks = 0, n_node_blocks = 0, n_ghost_blocks = 0;
+    int2 *cp_blocks = nullptr;  // kCpElemsPerBlock elements per block
+    int n_elem_blocks = 0, n_node_blocks = 0, n_ghost_blocks = 0, n_cp_blocks = 0;
 
     // mixed precision corner buffers
     lulesh::CornerF32 *dcorner32 = nullptr;
@@ -42,10 +43,14 @@ struct lulesh_set {
     void *arena = nullptr;
     size_t arena_bytes = 0;
 
-    // captured cycle
+    // captured cycle, and a graph of graph_cycles consecutive cycles
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     bool graph_ready = false;
+    int graph_cycles = 1;
+    cudaGraph_t graph_k = nullptr;
+    cudaGraphExec_t exec_k = nullptr;
+    bool graph_k_ready = false;
 
     // staged comm state: receive-buffer capacity per domain (doubles)
     long com_buf_doubles = 0;
@@ -68,6 +73,8 @@ void set_error(const std::string &msg);
 int cuda_status(cudaError_t e, const char *what);
 // enqueue one cycle (no graph)
 int enqueue_cycle(lulesh_set *s);
+// the FP64 force phase of every domain of the set
+void launch_force_fp64(lulesh_set *s, cudaStream_t st);
 // staged comm path of one cycle (comm.cu)
 int enqueue_cycle_staged(lulesh_set *s);
 // free the comm message tables of a set (comm.cu)

@@ -58,7 +58,26 @@ EXPORTED = [
     "lulesh_comm_recv", "lulesh_comm_send", "lulesh_comm_sbn",
     "lulesh_comm_sync_posvel", "lulesh_comm_monoq", "lulesh_comm_recv_offset",
     "lulesh_profile_phases", "lulesh_phase_name", "lulesh_volume_force_noalloc",
+    "lulesh_server_create", "lulesh_server_destroy", "lulesh_server_submit",
+    "lulesh_server_step", "lulesh_server_poll", "lulesh_server_clock",
+    "lulesh_set_graph_cycles",
 ]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_cap_bytes", ctypes.c_size_t), ("max_jobs", ctypes.c_int),
+                ("cycles_per_step", ctypes.c_int), ("prepare_threads", ctypes.c_int),
+                ("device", ctypes.c_int)]
+
+
+class ServerResult(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_longlong), ("status", ctypes.c_int), ("cycle", ctypes.c_int),
+                ("bad_elem", ctypes.c_int), ("origin_energy", ctypes.c_double),
+                ("time", ctypes.c_double), ("t_submit", ctypes.c_double),
+                ("t_admit", ctypes.c_double), ("t_done", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class Job(ctypes.Structure):
@@ -130,6 +149,13 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "lulesh_profile_phases": (ip, [vp, ip, ctypes.POINTER(dp), ctypes.POINTER(ip)]),
         "lulesh_phase_name": (ctypes.c_char_p, [ip]),
         "lulesh_volume_force_noalloc": (ip, [ip] + [vp] * 12 + [dp] + [vp] * 5),
+        "lulesh_server_create": (ip, [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]),
+        "lulesh_server_destroy": (ip, [vp]),
+        "lulesh_server_submit": (ip, [vp, ctypes.POINTER(Job), ctypes.POINTER(ctypes.c_longlong)]),
+        "lulesh_server_step": (ip, [vp, ctypes.POINTER(ip), ctypes.POINTER(ip)]),
+        "lulesh_server_poll": (ip, [vp, ctypes.POINTER(ServerResult), ip, ctypes.POINTER(ip)]),
+        "lulesh_server_clock": (dp, []),
+        "lulesh_set_graph_cycles": (ip, [vp, ip]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -226,6 +252,9 @@ class LuleshSet:
     def sync(self) -> None:
         _check(self.lib, self.lib.lulesh_sync(self.h), "lulesh_sync")
 
+    def set_graph_cycles(self, k: int) -> None:
+        _check(self.lib, self.lib.lulesh_set_graph_cycles(self.h, k), "lulesh_set_graph_cycles")
+
     def profile_phases(self, ncycles: int) -> dict:
         """Average ms per phase over `ncycles` separately launched cycles."""
         out = (ctypes.c_double * 12)()
@@ -318,3 +347,57 @@ class LuleshSet:
     def comm_recv_offset(self, recv_rank, dc, dr, dp, xfer, do_recv, plane_only) -> int:
         return int(self.lib.lulesh_comm_recv_offset(self.h, recv_rank, dc, dr, dp, xfer,
                                                     int(do_recv), int(plane_only)))
+
+
+class Server:
+    """Continuous-batching server (lulesh_server_*): submit jobs, call step()
+    repeatedly, poll() finished results."""
+
+    def __init__(self, hbm_cap_bytes: int = 150 * 10**9, max_jobs: int = 256,
+                 cycles_per_step: int = 8, prepare_threads: int = 4, device: int = -1):
+        self.lib = load_library()
+        cfg = ServerConfig(hbm_cap_bytes, max_jobs, cycles_per_step, prepare_threads, device)
+        h = ctypes.c_void_p()
+        _check(self.lib, self.lib.lulesh_server_create(ctypes.byref(cfg), ctypes.byref(h)),
+               "lulesh_server_create")
+        self.h = h
+
+    def submit(self, job: JobSpec) -> int:
+        jid = ctypes.c_longlong()
+        c = job.c()
+        _check(self.lib, self.lib.lulesh_server_submit(self.h, ctypes.byref(c), ctypes.byref(jid)),
+               "lulesh_server_submit")
+        return jid.value
+
+    def step(self) -> tuple[int, int]:
+        a, q = ctypes.c_int(), ctypes.c_int()
+        _check(self.lib, self.lib.lulesh_server_step(self.h, ctypes.byref(a), ctypes.byref(q)),
+               "lulesh_server_step")
+        return a.value, q.value
+
+    def poll(self, max_results: int = 1024) -> list[dict]:
+        buf = (ServerResult * max_results)()
+        n = ctypes.c_int()
+        _check(self.lib, self.lib.lulesh_server_poll(self.h, buf, max_results, ctypes.byref(n)),
+               "lulesh_server_poll")
+        return [buf[i].as_dict() for i in range(n.value)]
+
+    def clock(self) -> float:
+        return float(self.lib.lulesh_server_clock())
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.lulesh_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

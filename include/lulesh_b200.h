@@ -145,6 +145,11 @@ int lulesh_lagrange_leapfrog(lulesh_set *set);
 /* `ncycles` such cycles, asynchronously. */
 int lulesh_step(lulesh_set *set, int ncycles);
 
+/* Capture k consecutive cycles in one CUDA graph (default 1): lulesh_step(n)
+ * then issues n / k launches of the k-cycle graph and n % k of the
+ * one-cycle graph, so a whole batch run can be a single graph launch. */
+int lulesh_set_graph_cycles(lulesh_set *set, int k);
+
 /* The reference main loop (lulesh.cu:4858-4873): cycles until every job
  * has reached its cap or stoptime or failed, checking status every
  * `check_every` cycles (<= 0: 64).  Synchronous.  Returns LULESH_OK or the
@@ -202,6 +207,49 @@ int lulesh_write_solution(lulesh_set *set, int domain, const char *path);
 
 const char *lulesh_status_string(int status);
 const char *lulesh_last_error(void);
+
+/* ---- serving: continuous batching of sedov jobs ----------------------- */
+/* No reference counterpart (the reference runs one job per process).  A
+ * server owns one GPU stream.  Submitted jobs are meshed on host worker
+ * threads, admitted in arrival order while their device footprint
+ * (lulesh_footprint_bytes) fits under hbm_cap_bytes and a slot is free,
+ * and from then on keep their Domain state resident on the device.  Each
+ * lulesh_server_step advances every resident job by cycles_per_step cycles
+ * in one captured graph (jobs of different sizes share every launch),
+ * retires the jobs that finished (time >= stoptime, its reached, or an
+ * error) and admits new ones.  A job's result is bit-identical to running
+ * it alone with lulesh_create + lulesh_run. */
+typedef struct lulesh_server_config {
+    size_t hbm_cap_bytes; /* admission cap on the device memory of resident jobs */
+    int max_jobs;         /* resident jobs at most (slots), >= 1 */
+    int cycles_per_step;  /* cycles per lulesh_server_step, >= 1 */
+    int prepare_threads;  /* host threads that build submitted meshes, >= 1 */
+    int device;           /* < 0: current device */
+} lulesh_server_config;
+
+typedef struct lulesh_server_result {
+    long long id;          /* as returned by lulesh_server_submit */
+    int status;            /* LULESH_OK or VolumeError / QStopError */
+    int cycle;             /* cycles run */
+    int bad_elem;          /* element of the error, or -1 */
+    double origin_energy;  /* Final Origin Energy */
+    double time;           /* simulated time reached */
+    double t_submit, t_admit, t_done; /* host monotonic clock, seconds */
+} lulesh_server_result;
+
+typedef struct lulesh_server lulesh_server;
+
+int lulesh_server_create(const lulesh_server_config *cfg, lulesh_server **out);
+int lulesh_server_destroy(lulesh_server *srv);
+/* Queue a job (returns immediately; meshing starts on a worker thread). */
+int lulesh_server_submit(lulesh_server *srv, const lulesh_job *job, long long *id);
+/* Retire finished jobs, admit queued ones that fit, advance the resident
+ * ones.  *n_active / *n_queued (may be NULL) report the state after it. */
+int lulesh_server_step(lulesh_server *srv, int *n_active, int *n_queued);
+/* Move up to `max` finished results into out[]; *n receives the count. */
+int lulesh_server_poll(lulesh_server *srv, lulesh_server_result *out, int max, int *n);
+/* Host monotonic clock used for the t_* fields (seconds). */
+double lulesh_server_clock(void);
 
 /* ---- nodal forces without allocation --------------------------------- */
 /* No counterpart in the reference.  For callers that cannot allocate device

@@ -82,6 +82,73 @@ def test_setup_matches_oracle(host, oracle_mod, nx, tp, loc, rank, nr, b, c):
     assert dt[0] == o.scalar("initial_deltatime")
 
 
+def _face_links(z, nx, tp, col, row, plane, ghost):
+    """The rule the EOS kernel evaluates in place of elemBC/lxim..lzetap
+    (kernels.cu elem_face_links)."""
+    ix, iy, iz = z % nx, (z // nx) % nx, z // (nx * nx)
+    bc = 0
+    l = [z - 1, z + 1, z - nx, z + nx, z - nx * nx, z + nx * nx]  # xm xp em ep zm zp
+    last = tp - 1
+    if iz == 0:
+        if plane == 0:
+            bc |= 0x01000
+        else:
+            bc |= 0x04000; l[4] = ghost[0] + iy * nx + ix
+    if iz == nx - 1:
+        if plane == last:
+            bc |= 0x10000
+        else:
+            bc |= 0x20000; l[5] = ghost[1] + iy * nx + ix
+    if iy == 0:
+        if row == 0:
+            bc |= 0x00040
+        else:
+            bc |= 0x00100; l[2] = ghost[2] + iz * nx + ix
+    if iy == nx - 1:
+        if row == last:
+            bc |= 0x00400
+        else:
+            bc |= 0x00800; l[3] = ghost[3] + iz * nx + ix
+    if ix == 0:
+        if col == 0:
+            bc |= 0x00001
+        else:
+            bc |= 0x00004; l[0] = ghost[4] + iz * nx + iy
+    if ix == nx - 1:
+        if col == last:
+            bc |= 0x00010
+        else:
+            bc |= 0x00020; l[1] = ghost[5] + iz * nx + iy
+    return bc, l
+
+
+@pytest.mark.parametrize("nx,tp,loc", [(5, 1, (0, 0, 0)), (4, 2, (1, 0, 1)), (3, 3, (1, 1, 1)),
+                                       (4, 3, (0, 2, 1)), (1, 2, (1, 1, 1))])
+def test_face_link_rule_matches_connectivity(oracle_mod, nx, tp, loc):
+    """Where the limiter reads a neighbour (masks other than SYMM/FREE), the
+    arithmetic rule gives exactly the SetupConnectivityBC index."""
+    col, row, plane = loc
+    o = oracle_mod.Oracle(nx, tp=tp, col=col, row=row, plane=plane)
+    bcs = o.field("elemBC")
+    names = ["lxim", "lxip", "letam", "letap", "lzetam", "lzetap"]
+    arrs = [o.field(n) for n in names]
+    E = nx ** 3
+    present = [plane > 0, plane < tp - 1, row > 0, row < tp - 1, col > 0, col < tp - 1]
+    ghost, p = [], E
+    for f in range(6):
+        ghost.append(p if present[f] else -1)
+        p += nx * nx if present[f] else 0
+    # (mask of the face, symm bit, free bit) per neighbour slot
+    faces = [(0x7, 0x1, 0x2), (0x38, 0x8, 0x10), (0x1C0, 0x40, 0x80), (0xE00, 0x200, 0x400),
+             (0x7000, 0x1000, 0x2000), (0x38000, 0x8000, 0x10000)]
+    for z in range(E):
+        bc, l = _face_links(z, nx, tp, col, row, plane, ghost)
+        assert bc == bcs[z], z
+        for s, (mask, symm, free) in enumerate(faces):
+            if (bc & mask) not in (symm, free):
+                assert l[s] == arrs[s][z], (z, names[s])
+
+
 def test_global_nodal_mass_equals_undecomposed(host):
     """With global-order summation a subdomain's nodal masses equal the
     matching nodes of the undecomposed mesh bit for bit."""
