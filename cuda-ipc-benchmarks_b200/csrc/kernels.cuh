@@ -25,12 +25,6 @@ constexpr int kNodeBlock = 128;  // threads per block, node kernels
 #ifndef LULESH_EOS_MINB
 #define LULESH_EOS_MINB 8
 #endif
-// Velocity gathers of the force and kinematics kernels: 0 where the
-// arithmetic first needs them, 1 prefetched into L1 at kernel start,
-// 2 prefetched into L2 at kernel start, 3 loaded into registers at start.
-#ifndef LULESH_VEL_PREFETCH
-#define LULESH_VEL_PREFETCH 0
-#endif
 constexpr int kForceCpMinBlocks = LULESH_FORCECP_MINB;
 constexpr int kForceMinBlocks = LULESH_FORCE_MINB;
 constexpr int kKinMinBlocks = LULESH_KIN_MINB;

@@ -221,8 +221,7 @@ int lulesh_server_create(const lulesh_server_config *cfg, lulesh_server **out)
     int st;
     if (cfg->device >= 0 && (st = cuda_status(cudaSetDevice(cfg->device), "set device")))
         return fail(st);
-    if ((st = cuda_status(cudaGetDevice(&s->device), "get device"))) return fail(st);
-    if ((st = cuda_status(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream")))
+    if ((st = cuda_status(cudaGetDevice(&s->device), "get device"))) return fail(st);    if ((st = cuda_status(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream")))
         return fail(st);
     if ((st = cuda_status(cudaStreamCreateWithFlags(&s->upload, cudaStreamNonBlocking), "stream")))
         return fail(st);

@@ -88,8 +88,7 @@ struct DomPlace {
 static int create_common(lulesh_set *s, const std::vector<DomPlace> &place, int device)
 {
     if (device >= 0) LCHECK(cudaSetDevice(device));
-    LCHECK(cudaGetDevice(&s->device));
-    if (!s->stream) {
+    LCHECK(cudaGetDevice(&s->device));    if (!s->stream) {
         LCHECK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
         s->own_stream = true;
     }
