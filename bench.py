@@ -19,6 +19,16 @@ the total over ranks using the max time over ranks.
 
 --impl reference times the reference's own OpenMP CPU build
 (oracle/_ref/lulesh_omp, compiled from LULESH/omp_4.0) on this host's cores.
+
+At one GPU the line also carries the two other halves of the metric:
+  serving  a seeded Poisson stream of sedov jobs (lambda 50/s, edge
+           log-uniform in [8,64], regions U[5,20], iterations U[100,2000];
+           --serve-jobs of the 2,000-job stream, default 300) served with
+           continuous batching vs the same stream run job by job through the
+           plain path: zone-cycles/s over the makespan, p50/p99 job latency
+           (completion - arrival, wall clock), energies compared per job
+  batch    the 64-job batch (rng seed 0) in one graph stream with autotuned
+           launch shapes vs each job's own plain run (device time)
 """
 import argparse
 import json
@@ -264,6 +274,20 @@ def run_ours(a, rank, world, local_rank):
         dist.destroy_process_group()
     if rank != 0:
         return
+    serving_res = batch_res = None
+    if world == 1 and a.serve_jobs > 0:
+        import serving
+
+        stream_jobs = serving.make_stream(n_jobs=2000)[:a.serve_jobs]
+        cmp = serving.compare(stream_jobs)
+        serving_res = {"jobs": a.serve_jobs, "of": 2000, "lambda_per_s": 50.0,
+                       "served": cmp["served"], "plain": cmp["plain"],
+                       "throughput_ratio": cmp["throughput_ratio"],
+                       "energy_mismatches": cmp["energy_mismatches"]}
+    if world == 1 and a.batch_jobs > 0:
+        import batching
+
+        batch_res = batching.run_batch_vs_plain(batching.config3_jobs(n=a.batch_jobs))
     cpu = cpu_baseline_sample() if world == 1 else None
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
@@ -289,6 +313,7 @@ def run_ours(a, rank, world, local_rank):
         "phases_ms": phases, "phases_sum_ms": step_ms_sum,
         "clocks": ck, "origin_energy": energy, "cycles_run": total,
         "cpu_baseline": cpu,
+        "serving": serving_res, "batch": batch_res,
     }
     print(json.dumps(line), flush=True)
 
@@ -333,6 +358,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--profile-cycles", dest="profile_cycles", type=int, default=5)
     ap.add_argument("--e2e-cycles", dest="e2e_cycles", type=int, default=100)
+    ap.add_argument("--serve-jobs", dest="serve_jobs", type=int, default=300,
+                    help="jobs of the serving stream (2000 = the full stream; 0 skips)")
+    ap.add_argument("--batch-jobs", dest="batch_jobs", type=int, default=64,
+                    help="jobs of the batch comparison (0 skips)")
     a = ap.parse_args()
     if a.warmup < 3:
         ap.error("--warmup must be >= 3")

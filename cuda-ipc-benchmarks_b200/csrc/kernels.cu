@@ -112,8 +112,8 @@ __device__ __constant__ int kCZ[8] = {0, 0, 0, 0, 1, 1, 1, 1};
 // ---------------------------------------------------------------------------
 // force: CalcVolumeForceForElems_kernel, lulesh.cu:2080-2259
 
-template <bool HG>
-__global__ void __launch_bounds__(kElemBlock, kForceMinBlocks) k_force(SetArgs a, Params P)
+template <bool HG, int BS>
+__global__ void __launch_bounds__(BS, min_blocks(kForceMinBlocks, BS)) k_force(SetArgs a, Params P)
 {
     const int2 blk = a.blocks[blockIdx.x];
     const DomDev &D = a.doms[blk.x];
@@ -127,7 +127,8 @@ __global__ void __launch_bounds__(kElemBlock, kForceMinBlocks) k_force(SetArgs a
     // hourglass step (measured on B200 at -s 100: 150 -> 136 us)
     int n[8];
     elem_nodes(D, elem, n);
-    double xn[8], yn[8], zn[8], xdn[8], ydn[8], zdn[8];
+    double xn[8], yn[8], zn[8];
+    double xdn[8], ydn[8], zdn[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         if (HG) {
@@ -138,21 +139,32 @@ __global__ void __launch_bounds__(kElemBlock, kForceMinBlocks) k_force(SetArgs a
             xdn[i] = ydn[i] = zdn[i] = 0.0;
         }
     }
+    const VelRegs vel{xdn, ydn, zdn};
 #pragma unroll
     for (int i = 0; i < 8; ++i) xn[i] = D.x[n[i]];
 #pragma unroll
     for (int i = 0; i < 8; ++i) yn[i] = D.y[n[i]];
 #pragma unroll
     for (int i = 0; i < 8; ++i) zn[i] = D.z[n[i]];
-    force_elem<HG>(D, T, P, elem, xn, yn, zn, xdn, ydn, zdn);
+    force_elem<HG>(D, T, P, elem, xn, yn, zn, vel);
 }
 
-void launch_force(const SetArgs &a, int nblocks, Params P, cudaStream_t s)
+template <int BS>
+static void launch_force_bs(const SetArgs &a, int nblocks, Params P, cudaStream_t s)
 {
     if (P.hgcoef > 0.0)
-        k_force<true><<<nblocks, kElemBlock, 0, s>>>(a, P);
+        k_force<true, BS><<<nblocks, BS, 0, s>>>(a, P);
     else
-        k_force<false><<<nblocks, kElemBlock, 0, s>>>(a, P);
+        k_force<false, BS><<<nblocks, BS, 0, s>>>(a, P);
+}
+
+void launch_force(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs)
+{
+    switch (bs) {
+        case 64: launch_force_bs<64>(a, nblocks, P, s); break;
+        case 256: launch_force_bs<256>(a, nblocks, P, s); break;
+        default: launch_force_bs<kElemBlock>(a, nblocks, P, s); break;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -176,9 +188,9 @@ __device__ __forceinline__ void gather_corners(const DomDev *doms, const DomDev 
                             (unsigned)ez < (unsigned)nx;
         if (inside) {
             const int idx = j * D.Ep + (ez * nx + ey) * nx + ex;
-            fx += D.fx_elem[idx];
-            fy += D.fy_elem[idx];
-            fz += D.fz_elem[idx];
+            fx += ld_corner(D.fx_elem + idx);
+            fy += ld_corner(D.fy_elem + idx);
+            fz += ld_corner(D.fz_elem + idx);
         } else if (D.tp > 1) {
             const int sx = (ex < 0) ? -1 : (ex >= nx ? 1 : 0);
             const int sy = (ey < 0) ? -1 : (ey >= nx ? 1 : 0);
@@ -188,9 +200,9 @@ __device__ __forceinline__ void gather_corners(const DomDev *doms, const DomDev 
                 const DomDev &N = doms[nb];
                 const int lx = ex - sx * nx, ly = ey - sy * nx, lz = ez - sz * nx;
                 const int idx = j * N.Ep + (lz * nx + ly) * nx + lx;
-                fx += N.fx_elem[idx];
-                fy += N.fy_elem[idx];
-                fz += N.fz_elem[idx];
+                fx += ld_corner(N.fx_elem + idx);
+                fy += ld_corner(N.fy_elem + idx);
+                fz += ld_corner(N.fz_elem + idx);
             }
         }
     }
@@ -201,8 +213,8 @@ __device__ __forceinline__ void gather_corners(const DomDev *doms, const DomDev 
 // MODE 1: AddNodeForcesFromElems over this domain's own corners only,
 //         writing fx/fy/fz (the partial sums the reference exchanges).
 // MODE 2: the node update from fx/fy/fz (after CommSBN added neighbours).
-template <int MODE>
-__global__ void __launch_bounds__(kNodeBlock) k_nodal(SetArgs a, Params P)
+template <int MODE, int BS>
+__global__ void __launch_bounds__(BS) k_nodal(SetArgs a, Params P)
 {
     const int2 blk = a.blocks[blockIdx.x];
     const DomDev &D = a.doms[blk.x];
@@ -271,25 +283,30 @@ __global__ void __launch_bounds__(kNodeBlock) k_nodal(SetArgs a, Params P)
     }
 }
 
-void launch_nodal(const SetArgs &a, int nblocks, Params P, cudaStream_t s)
+void launch_nodal(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs)
 {
-    k_nodal<0><<<nblocks, kNodeBlock, 0, s>>>(a, P);
+    switch (bs) {
+        case 256: k_nodal<0, 256><<<nblocks, 256, 0, s>>>(a, P); break;
+        case 512: k_nodal<0, 512><<<nblocks, 512, 0, s>>>(a, P); break;
+        default: k_nodal<0, kNodeBlock><<<nblocks, kNodeBlock, 0, s>>>(a, P); break;
+    }
 }
 
 void launch_nodal_gather_local(const SetArgs &a, int nblocks, cudaStream_t s)
 {
-    k_nodal<1><<<nblocks, kNodeBlock, 0, s>>>(a, Params{});
+    k_nodal<1, kNodeBlock><<<nblocks, kNodeBlock, 0, s>>>(a, Params{});
 }
 
 void launch_nodal_update(const SetArgs &a, int nblocks, Params P, cudaStream_t s)
 {
-    k_nodal<2><<<nblocks, kNodeBlock, 0, s>>>(a, P);
+    k_nodal<2, kNodeBlock><<<nblocks, kNodeBlock, 0, s>>>(a, P);
 }
 
 // ---------------------------------------------------------------------------
 // kinematics: CalcKinematicsAndMonotonicQGradient_kernel, lulesh.cu:3343-3507
 
-__global__ void __launch_bounds__(kElemBlock, kKinMinBlocks) k_kinematics(SetArgs a, Params P)
+template <int BS>
+__global__ void __launch_bounds__(BS, min_blocks(kKinMinBlocks, BS)) k_kinematics(SetArgs a)
 {
     const int2 blk = a.blocks[blockIdx.x];
     const DomDev &D = a.doms[blk.x];
@@ -309,18 +326,24 @@ __global__ void __launch_bounds__(kElemBlock, kKinMinBlocks) k_kinematics(SetArg
         yd_local[l] = D.yd[nodes[l]];
         zd_local[l] = D.zd[nodes[l]];
     }
+    const VelRegs vel{xd_local, yd_local, zd_local};
 #pragma unroll
     for (int l = 0; l < 8; ++l) x_local[l] = D.x[nodes[l]];
 #pragma unroll
     for (int l = 0; l < 8; ++l) y_local[l] = D.y[nodes[l]];
 #pragma unroll
     for (int l = 0; l < 8; ++l) z_local[l] = D.z[nodes[l]];
-    kin_elem(D, T, k, x_local, y_local, z_local, xd_local, yd_local, zd_local);
+    kin_elem(D, T, k, x_local, y_local, z_local, vel);
 }
 
-void launch_kinematics(const SetArgs &a, int nblocks, Params P, cudaStream_t s)
+void launch_kinematics(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs)
 {
-    k_kinematics<<<nblocks, kElemBlock, 0, s>>>(a, P);
+    (void)P;
+    switch (bs) {
+        case 64: k_kinematics<64><<<nblocks, 64, 0, s>>>(a); break;
+        case 256: k_kinematics<256><<<nblocks, 256, 0, s>>>(a); break;
+        default: k_kinematics<kElemBlock><<<nblocks, kElemBlock, 0, s>>>(a); break;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -488,7 +511,8 @@ __device__ __forceinline__ double warp_min(double v)
     return v;
 }
 
-__global__ void __launch_bounds__(kElemBlock, kEosMinBlocks) k_eos(SetArgs a, Params P)
+template <int BS>
+__global__ void __launch_bounds__(BS, min_blocks(kEosMinBlocks, BS)) k_eos(SetArgs a, Params P)
 {
     const int2 blk = a.blocks[blockIdx.x];
     const DomDev &D = a.doms[blk.x];
@@ -638,7 +662,7 @@ __global__ void __launch_bounds__(kElemBlock, kEosMinBlocks) k_eos(SetArgs a, Pa
         if (vdov_tmp != 0. && dtf < dtc) dtc = dtf;
     }
     // block minimum (exact, order-free), one atomic per block
-    __shared__ double s_c[kElemBlock / 32], s_h[kElemBlock / 32];
+    __shared__ double s_c[BS / 32], s_h[BS / 32];
     dtc = warp_min(dtc);
     dth = warp_min(dth);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -650,7 +674,7 @@ __global__ void __launch_bounds__(kElemBlock, kEosMinBlocks) k_eos(SetArgs a, Pa
     if (threadIdx.x == 0) {
         double c = s_c[0], h = s_h[0];
 #pragma unroll
-        for (int w = 1; w < kElemBlock / 32; ++w) {
+        for (int w = 1; w < BS / 32; ++w) {
             c = fmin(c, s_c[w]);
             h = fmin(h, s_h[w]);
         }
@@ -659,9 +683,13 @@ __global__ void __launch_bounds__(kElemBlock, kEosMinBlocks) k_eos(SetArgs a, Pa
     }
 }
 
-void launch_eos(const SetArgs &a, int nblocks, Params P, cudaStream_t s)
+void launch_eos(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs)
 {
-    k_eos<<<nblocks, kElemBlock, 0, s>>>(a, P);
+    switch (bs) {
+        case 64: k_eos<64><<<nblocks, 64, 0, s>>>(a, P); break;
+        case 256: k_eos<256><<<nblocks, 256, 0, s>>>(a, P); break;
+        default: k_eos<kElemBlock><<<nblocks, kElemBlock, 0, s>>>(a, P); break;
+    }
 }
 
 // ---------------------------------------------------------------------------

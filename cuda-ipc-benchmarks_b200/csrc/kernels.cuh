@@ -30,6 +30,18 @@ constexpr int kForceMinBlocks = LULESH_FORCE_MINB;
 constexpr int kKinMinBlocks = LULESH_KIN_MINB;
 constexpr int kEosMinBlocks = LULESH_EOS_MINB;
 
+// Minimum resident blocks of a kernel launched with BS threads per block
+// that keeps the per-SM thread target of `minb` blocks of 128 threads.
+constexpr int min_blocks(int minb, int bs)
+{
+    return (minb * 128 / bs) > 0 ? (minb * 128 / bs) : 1;
+}
+
+// Block shapes the FP64 element kernels (force, kinematics, EOS) and the
+// nodal kernel are compiled for; a set's block tables use one of each.
+constexpr bool valid_elem_block(int bs) { return bs == 64 || bs == 128 || bs == 256; }
+constexpr bool valid_node_block(int bs) { return bs == 128 || bs == 256 || bs == 512; }
+
 // A kernel launch over all domains of a set: block b works on domain
 // blocks[b].x starting at item blocks[b].y (element, node or region slot).
 struct SetArgs {
@@ -40,7 +52,8 @@ struct SetArgs {
 };
 
 void launch_time_increment(TimeCtl *tcs, int ntc, Params P, cudaStream_t s);
-void launch_force(const SetArgs &a, int nblocks, Params P, cudaStream_t s);
+void launch_force(const SetArgs &a, int nblocks, Params P, cudaStream_t s,
+                  int bs = kElemBlock);
 // corner-parallel force kernel: 8 threads per element, kCpElemsPerBlock
 // elements per block (blocks[] built with that step)
 constexpr int kCpElemsPerBlock = 32;
@@ -49,12 +62,14 @@ void launch_force_cp(const SetArgs &a, int nblocks, Params P, cudaStream_t s);
 #ifndef LULESH_FORCE_CP
 #define LULESH_FORCE_CP 0
 #endif
-void launch_nodal(const SetArgs &a, int nblocks, Params P, cudaStream_t s);
+void launch_nodal(const SetArgs &a, int nblocks, Params P, cudaStream_t s,
+                  int bs = kNodeBlock);
 // staged comm path: own-corner partial sums, then the update from fx/fy/fz
 void launch_nodal_gather_local(const SetArgs &a, int nblocks, cudaStream_t s);
 void launch_nodal_update(const SetArgs &a, int nblocks, Params P, cudaStream_t s);
-void launch_kinematics(const SetArgs &a, int nblocks, Params P, cudaStream_t s);
-void launch_eos(const SetArgs &a, int nblocks, Params P, cudaStream_t s);
+void launch_kinematics(const SetArgs &a, int nblocks, Params P, cudaStream_t s,
+                       int bs = kElemBlock);
+void launch_eos(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs = kElemBlock);
 // fused halo kernels of a subdomain set (direct reads of neighbour memory)
 void launch_posvel_sync(const SetArgs &a, int nblocks, cudaStream_t s);
 void launch_monoq_ghost(const SetArgs &a, int nblocks, cudaStream_t s);

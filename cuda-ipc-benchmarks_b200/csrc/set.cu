@@ -1,4 +1,5 @@
 // set.cu -- lifetime, stepping and results of a lulesh_set (the C ABI).
+#include <algorithm>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -42,14 +43,22 @@ static int validate_job(const lulesh_job &j)
     return LULESH_OK;
 }
 
-static int build_tables(lulesh_set *s)
+int build_tables(lulesh_set *s)
 {
+    // domains in creation order, or largest first: big domains then start
+    // their blocks first and small ones fill the tail of each launch
+    std::vector<int> dord(s->ndom);
+    for (int d = 0; d < s->ndom; ++d) dord[d] = d;
+    if (s->order == 1)
+        std::stable_sort(dord.begin(), dord.end(), [s](int a, int b) {
+            return s->hdoms[a].numElem > s->hdoms[b].numElem;
+        });
     std::vector<int2> eb, nb, gb, cb;
-    for (int d = 0; d < s->ndom; ++d) {
+    for (int d : dord) {
         const DomDev &D = s->hdoms[d];
-        for (int i = 0; i < D.numElem; i += kElemBlock) eb.push_back(make_int2(d, i));
+        for (int i = 0; i < D.numElem; i += s->eb) eb.push_back(make_int2(d, i));
         for (int i = 0; i < D.numElem; i += kCpElemsPerBlock) cb.push_back(make_int2(d, i));
-        for (int i = 0; i < D.numNode; i += kNodeBlock) nb.push_back(make_int2(d, i));
+        for (int i = 0; i < D.numNode; i += s->nb) nb.push_back(make_int2(d, i));
         if (D.tp > 1)
             for (int f = 0; f < 6; ++f)
                 if (D.ghost[f] >= 0)
@@ -61,6 +70,11 @@ static int build_tables(lulesh_set *s)
     s->n_ghost_blocks = (int)gb.size();
     s->n_cp_blocks = (int)cb.size();
     size_t bytes = sizeof(int2) * (eb.size() + nb.size() + gb.size() + cb.size() + 1);
+    if (s->elem_blocks) {  // rebuilding: the old tables may still be in use
+        LCHECK(cudaStreamSynchronize(s->stream));
+        LCHECK(cudaFree(s->elem_blocks));
+        s->elem_blocks = nullptr;
+    }
     int2 *t = nullptr;
     LCHECK(cudaMalloc(&t, bytes));
     s->elem_blocks = t;
@@ -88,7 +102,8 @@ struct DomPlace {
 static int create_common(lulesh_set *s, const std::vector<DomPlace> &place, int device)
 {
     if (device >= 0) LCHECK(cudaSetDevice(device));
-    LCHECK(cudaGetDevice(&s->device));    if (!s->stream) {
+    LCHECK(cudaGetDevice(&s->device));
+    if (!s->stream) {
         LCHECK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
         s->own_stream = true;
     }
@@ -174,7 +189,7 @@ void launch_force_fp64(lulesh_set *s, cudaStream_t st)
 #if LULESH_FORCE_CP
     launch_force_cp(s->args(s->cp_blocks), s->n_cp_blocks, s->P, st);
 #else
-    launch_force(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st);
+    launch_force(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb);
 #endif
 }
 
@@ -191,15 +206,15 @@ int enqueue_cycle(lulesh_set *s)
     if (mixed)
         launch_nodal_mixed(s->args(s->node_blocks), s->n_node_blocks, s->P, s->dcorner32, st);
     else
-        launch_nodal(s->args(s->node_blocks), s->n_node_blocks, s->P, st);
+        launch_nodal(s->args(s->node_blocks), s->n_node_blocks, s->P, st, s->nb);
     if (s->tp > 1) launch_posvel_sync(s->args(s->node_blocks), s->n_node_blocks, st);
     if (mixed)
         launch_kinematics_mixed(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st);
     else
-        launch_kinematics(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st);
+        launch_kinematics(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb);
     if (s->tp > 1 && s->n_ghost_blocks > 0)
         launch_monoq_ghost(s->args(s->ghost_blocks), s->n_ghost_blocks, st);
-    launch_eos(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st);
+    launch_eos(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb);
     return cuda_status(cudaGetLastError(), "cycle launch");
 }
 
@@ -246,7 +261,7 @@ static int ensure_graph_k(lulesh_set *s)
     return LULESH_OK;
 }
 
-static void drop_graph(lulesh_set *s)
+void drop_graph(lulesh_set *s)
 {
     if (s->exec_k) cudaGraphExecDestroy(s->exec_k);
     if (s->graph_k) cudaGraphDestroy(s->graph_k);
@@ -599,19 +614,19 @@ int lulesh_profile_phases(lulesh_set *s, int ncycles, double *ms_out, int *nphas
         if (mixed)
             launch_nodal_mixed(s->args(s->node_blocks), s->n_node_blocks, s->P, s->dcorner32, st);
         else
-            launch_nodal(s->args(s->node_blocks), s->n_node_blocks, s->P, st);
+            launch_nodal(s->args(s->node_blocks), s->n_node_blocks, s->P, st, s->nb);
         LCHECK(cudaEventRecord(ev[3], st));
         if (s->tp > 1) launch_posvel_sync(s->args(s->node_blocks), s->n_node_blocks, st);
         LCHECK(cudaEventRecord(ev[4], st));
         if (mixed)
             launch_kinematics_mixed(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st);
         else
-            launch_kinematics(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st);
+            launch_kinematics(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb);
         LCHECK(cudaEventRecord(ev[5], st));
         if (s->tp > 1 && s->n_ghost_blocks > 0)
             launch_monoq_ghost(s->args(s->ghost_blocks), s->n_ghost_blocks, st);
         LCHECK(cudaEventRecord(ev[6], st));
-        launch_eos(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st);
+        launch_eos(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb);
         LCHECK(cudaEventRecord(ev[7], st));
         LCHECK(cudaEventSynchronize(ev[7]));
         for (int k = 0; k < np; ++k) {

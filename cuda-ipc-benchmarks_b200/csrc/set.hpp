@@ -28,7 +28,12 @@ struct lulesh_set {
     std::vector<lulesh_job> jobs;
     std::vector<size_t> corner_list_len;
 
-    // device tables
+    // block shapes and block-table order (lulesh_set_tuning): elements per
+    // block of the FP64 element kernels, nodes per block of the nodal
+    // kernel, 0 = domains in creation order / 1 = largest domain first
+    int eb = lulesh::kElemBlock, nb = lulesh::kNodeBlock, order = 0;
+
+    // device tables (elem_blocks is the base of one allocation holding all)
     lulesh::DomDev *ddoms = nullptr;
     lulesh::TimeCtl *dtc = nullptr;
     lulesh::TimeCtl *htc_pinned = nullptr;  // pinned mirror for readback
@@ -81,4 +86,8 @@ int enqueue_cycle_staged(lulesh_set *s);
 void comm_release(const lulesh_set *s);
 // allocate the staged cycle's message tables ahead of graph capture
 int comm_prepare(lulesh_set *s);
+// (re)build the block tables from s->eb, s->nb, s->order
+int build_tables(lulesh_set *s);
+// release the captured cycle graphs (rebuilt at the next step)
+void drop_graph(lulesh_set *s);
 }  // namespace lulesh

@@ -60,7 +60,8 @@ EXPORTED = [
     "lulesh_profile_phases", "lulesh_phase_name", "lulesh_volume_force_noalloc",
     "lulesh_server_create", "lulesh_server_destroy", "lulesh_server_submit",
     "lulesh_server_step", "lulesh_server_poll", "lulesh_server_clock",
-    "lulesh_set_graph_cycles",
+    "lulesh_set_graph_cycles", "lulesh_get_tuning", "lulesh_set_tuning",
+    "lulesh_autotune",
 ]
 
 
@@ -78,6 +79,18 @@ class ServerResult(ctypes.Structure):
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("elem_block", ctypes.c_int), ("node_block", ctypes.c_int),
+                ("order", ctypes.c_int), ("graph_cycles", ctypes.c_int)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class TuneTrial(ctypes.Structure):
+    _fields_ = [("tuning", Tuning), ("ms_per_cycle", ctypes.c_double)]
 
 
 class Job(ctypes.Structure):
@@ -156,6 +169,10 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "lulesh_server_poll": (ip, [vp, ctypes.POINTER(ServerResult), ip, ctypes.POINTER(ip)]),
         "lulesh_server_clock": (dp, []),
         "lulesh_set_graph_cycles": (ip, [vp, ip]),
+        "lulesh_get_tuning": (ip, [vp, ctypes.POINTER(Tuning)]),
+        "lulesh_set_tuning": (ip, [vp, ctypes.POINTER(Tuning)]),
+        "lulesh_autotune": (ip, [vp, ip, ip, ctypes.POINTER(Tuning), ctypes.POINTER(TuneTrial),
+                                 ip, ctypes.POINTER(ip)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -254,6 +271,29 @@ class LuleshSet:
 
     def set_graph_cycles(self, k: int) -> None:
         _check(self.lib, self.lib.lulesh_set_graph_cycles(self.h, k), "lulesh_set_graph_cycles")
+
+    def tuning(self) -> dict:
+        t = Tuning()
+        _check(self.lib, self.lib.lulesh_get_tuning(self.h, ctypes.byref(t)), "lulesh_get_tuning")
+        return t.as_dict()
+
+    def set_tuning(self, elem_block: int = 128, node_block: int = 128, order: int = 0,
+                   graph_cycles: int = 1) -> None:
+        t = Tuning(elem_block, node_block, order, graph_cycles)
+        _check(self.lib, self.lib.lulesh_set_tuning(self.h, ctypes.byref(t)), "lulesh_set_tuning")
+
+    def autotune(self, trial_cycles: int = 10, rounds: int = 2) -> dict:
+        """Time the candidate launch shapes from the current state (which is
+        restored afterwards) and apply the fastest; returns the winner and
+        every trial."""
+        best = Tuning()
+        trials = (TuneTrial * 64)()
+        n = ctypes.c_int(0)
+        _check(self.lib, self.lib.lulesh_autotune(self.h, trial_cycles, rounds, ctypes.byref(best),
+                                                  trials, 64, ctypes.byref(n)), "lulesh_autotune")
+        return {"best": best.as_dict(),
+                "trials": [dict(trials[i].tuning.as_dict(), ms_per_cycle=trials[i].ms_per_cycle)
+                           for i in range(n.value)]}
 
     def profile_phases(self, ncycles: int) -> dict:
         """Average ms per phase over `ncycles` separately launched cycles."""

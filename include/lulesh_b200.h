@@ -150,6 +150,40 @@ int lulesh_step(lulesh_set *set, int ncycles);
  * one-cycle graph, so a whole batch run can be a single graph launch. */
 int lulesh_set_graph_cycles(lulesh_set *set, int k);
 
+/* Launch shapes of a set.  No reference counterpart (the reference launches
+ * fixed 64/128-thread blocks per kernel); results do not depend on them. */
+typedef struct lulesh_tuning {
+    int elem_block;   /* elements (threads) per block of the FP64 force,
+                         kinematics and EOS kernels: 64, 128 or 256 */
+    int node_block;   /* nodes (threads) per block of the nodal kernel:
+                         128, 256 or 512 */
+    int order;        /* block tables: 0 domains in creation order,
+                         1 largest domain first */
+    int graph_cycles; /* cycles per graph launch, >= 1 */
+} lulesh_tuning;
+
+typedef struct lulesh_tune_trial {
+    lulesh_tuning tuning;
+    double ms_per_cycle; /* best of the rounds, device time */
+} lulesh_tune_trial;
+
+int lulesh_get_tuning(const lulesh_set *set, lulesh_tuning *out);
+
+/* Apply launch shapes.  Sets of subdomains (tp > 1), staged-comm and mixed
+ * precision sets take only elem_block = node_block = 128.
+ * LULESH_INVALID_ARG for a shape outside the lists above. */
+int lulesh_set_tuning(lulesh_set *set, const lulesh_tuning *tuning);
+
+/* Autotuner (no reference counterpart): saves the set's device state,
+ * times every candidate shape for `trial_cycles` cycles from that same state
+ * (`rounds` times each, interleaved; best kept), first over elem_block x
+ * node_block x order at one cycle per launch, then graph_cycles in
+ * {1, 2, 4, 8, 16} for the winner; restores the state and applies the
+ * fastest.  Synchronous; needs device memory for one copy of the set's
+ * state.  The trials (up to max_trials) are written to `trials`. */
+int lulesh_autotune(lulesh_set *set, int trial_cycles, int rounds, lulesh_tuning *best,
+                    lulesh_tune_trial *trials, int max_trials, int *n_trials);
+
 /* The reference main loop (lulesh.cu:4858-4873): cycles until every job
  * has reached its cap or stoptime or failed, checking status every
  * `check_every` cycles (<= 0: 64).  Synchronous.  Returns LULESH_OK or the

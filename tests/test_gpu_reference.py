@@ -1,0 +1,67 @@
+"""Parity with the reference's own results at full problem sizes.
+
+* cuda_reference.json: the reference CUDA single-domain build run on a B200
+  (tests/golden/make_golden_cuda.py).  Gate: Final Origin Energy within
+  1e-9 relative, same cycle count.
+* published_kats.json: energies published in the reference repository
+  (7 significant digits), from 8-rank runs of -s n, run here as one domain of
+  edge 2n.  Gate: 5e-7 relative (half a unit in the 7th digit).
+* Config 2: -s 100 as one domain and as 2x2x2 in-device subdomains of -s 50,
+  500 cycles: equal bit for bit, and within 1e-9 of the reference build.
+"""
+import json
+import os
+
+import pytest
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+
+def _load(name):
+    path = os.path.join(GOLDEN, name)
+    if not os.path.exists(path):
+        return {}
+    with open(path) as f:
+        return json.load(f)
+
+
+CUDA_REF = _load("cuda_reference.json").get("runs", {})
+KATS = _load("published_kats.json").get("runs", [])
+
+
+def _run(lulesh, nx, its, tp=1):
+    with lulesh.LuleshSet(nx=nx, tp=tp, its=its) as s:
+        st = s.run()
+        return st, s.origin_energy(), s.state()["cycle"], s.symmetry()
+
+
+@pytest.mark.parametrize("key", sorted(CUDA_REF), ids=str)
+def test_matches_reference_cuda_build(lulesh, key):
+    ref = CUDA_REF[key]
+    st, e, cycles, sym = _run(lulesh, ref["nx"], ref["its"])
+    assert st == lulesh.OK
+    assert cycles == ref["cycles"]
+    assert abs(e - ref["energy"]) <= 1e-9 * abs(ref["energy"]), (e, ref["energy"])
+    # plane-0 symmetry is as good as the reference's own
+    assert sym[2] <= max(10 * ref["max_rel"], 1e-12)
+
+
+@pytest.mark.parametrize("kat", KATS, ids=lambda k: f"s{k['nx']}_i{k['its']}")
+def test_published_known_answers(lulesh, kat):
+    st, e, cycles, _ = _run(lulesh, kat["nx"], kat["its"])
+    assert st == lulesh.OK
+    if "cycles" in kat:
+        assert cycles == kat["cycles"]
+    assert abs(e - kat["energy"]) <= 5e-7 * abs(kat["energy"]), (e, kat["energy"])
+
+
+def test_config2_subdomains_full_size(lulesh):
+    _, e1, c1, _ = _run(lulesh, 100, 500)
+    _, e8, c8, _ = _run(lulesh, 50, 500, tp=2)
+    assert c1 == c8 == 500
+    assert e1 == e8
+    ref = CUDA_REF.get("-s 100 -i 500")
+    if ref:
+        assert abs(e1 - ref["energy"]) <= 1e-9 * abs(ref["energy"])
