@@ -1,0 +1,36 @@
+"""Mixed precision (LULESH_FLAG_MIXED): element stress / hourglass /
+kinematics arithmetic in FP32 with compensated FP32 corner sums; EOS, node
+update and dt in FP64.  The error is stated against the FP64 run of the same
+problem, which itself matches the reference CUDA build to 1e-9."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(lulesh, nx, its, flags):
+    with lulesh.LuleshSet(nx=nx, its=its, flags=flags) as s:
+        st = s.run()
+        return st, s.origin_energy(), s.state()["cycle"], s.symmetry(), s.field("e")
+
+
+@pytest.mark.parametrize("nx,its,tol", [(30, 300, 1e-5), (120, 1000, 1e-6)])
+def test_mixed_precision_error_against_fp64(lulesh, nx, its, tol):
+    st64, e64, c64, sym64, f64 = _run(lulesh, nx, its, 0)
+    st32, e32, c32, sym32, f32 = _run(lulesh, nx, its, lulesh.FLAG_MIXED)
+    assert st64 == st32 == lulesh.OK
+    assert c32 == c64 == its
+    assert abs(e32 - e64) <= tol * abs(e64), (e32, e64)
+    # the energy field as a whole stays close where the energy is not tiny
+    big = np.abs(f64) > 1e-6 * np.abs(f64).max()
+    rel = np.abs(f32[big] - f64[big]) / np.abs(f64[big])
+    assert np.percentile(rel, 99) < 1e-3
+    # plane-0 symmetry: absolute asymmetry far below the origin energy
+    assert sym32[0] < 1e-6 * abs(e64)
+
+
+def test_mixed_precision_is_deterministic(lulesh):
+    a = _run(lulesh, 20, 100, lulesh.FLAG_MIXED)
+    b = _run(lulesh, 20, 100, lulesh.FLAG_MIXED)
+    assert a[1] == b[1]
+    assert (a[4] == b[4]).all()

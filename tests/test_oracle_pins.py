@@ -71,3 +71,20 @@ def test_oracle_step_is_deterministic(oracle_mod):
     b = oracle_mod.Oracle(9)
     b.run(25)
     assert np.array_equal(a.field("x"), b.field("x"))
+
+
+def _cuda_gold():
+    with open(os.path.join(GOLDEN, "cuda_reference.json")) as f:
+        return json.load(f)["runs"]
+
+
+@pytest.mark.parametrize("key", ["-s 10 -i 50", "-s 30 -i 100"])
+def test_oracle_matches_reference_cuda_build(oracle_mod, key):
+    """The reference CUDA build's own results (tests/golden/cuda_reference.json,
+    17 digits, one B200): the oracle follows its corner-order nodal sum, so
+    only FMA contraction separates them."""
+    gold = _cuda_gold()[key]
+    o = oracle_mod.Oracle(gold["nx"])
+    st, n = o.run(gold["its"])
+    assert st == 0 and n == gold["cycles"]
+    assert rel(o.origin_energy(), gold["energy"]) < 1e-12
