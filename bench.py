@@ -281,8 +281,9 @@ def run_ours(a, rank, world, local_rank):
         stream_jobs = serving.make_stream(n_jobs=2000)[:a.serve_jobs]
         cmp = serving.compare(stream_jobs)
         serving_res = {"jobs": a.serve_jobs, "of": 2000, "lambda_per_s": 50.0,
-                       "served": cmp["served"], "plain": cmp["plain"],
-                       "throughput_ratio": cmp["throughput_ratio"],
+                       "served": cmp["served"], "served_saturated": cmp["served_saturated"],
+                       "plain": cmp["plain"], "throughput_ratio": cmp["throughput_ratio"],
+                       "capacity_ratio": cmp["capacity_ratio"],
                        "energy_mismatches": cmp["energy_mismatches"]}
     if world == 1 and a.batch_jobs > 0:
         import batching

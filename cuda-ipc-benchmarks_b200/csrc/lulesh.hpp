@@ -58,7 +58,13 @@ class DomainSet {
         check(lulesh_create(&j, tp, flags, device, &set_), "NewDomain");
         tp_ = tp;
     }
-    ~DomainSet() { lulesh_destroy(set_); }
+    ~DomainSet() { release(); }
+    // free every device resource now (the destructor then does nothing)
+    void release()
+    {
+        if (set_) lulesh_destroy(set_);
+        set_ = nullptr;
+    }
     DomainSet(const DomainSet &) = delete;
     DomainSet &operator=(const DomainSet &) = delete;
     lulesh_set *get() const { return set_; }

@@ -5,13 +5,15 @@
 //   1. waits for the previous step, reads every slot's time control and
 //      origin energy (one gather kernel + two small copies issued at the end
 //      of that step) and retires finished jobs, freeing their memory;
-//   2. admits queued jobs in arrival order while a slot is free and the
-//      job's device footprint fits under the cap (stream-ordered
-//      allocations from a memory pool, uploaded on a side stream);
-//   3. when the resident set changed, rebuilds the domain table and block
-//      tables and re-captures the cycle graph;
-//   4. launches the cycle graph cycles_per_step times: every resident job,
-//      whatever its size, advances in the same five launches per cycle.
+//   2. when the resident set changed, rebuilds the domain table and block
+//      tables, writes the time state of newly admitted jobs and re-captures
+//      the cycle graph (updating the executable graph in place);
+//   3. launches the cycle graph cycles_per_step times: every resident job,
+//      whatever its size, advances in the same five launches per cycle;
+//   4. while those cycles run, admits queued jobs in arrival order while a
+//      slot is free and the job's device footprint fits under the cap
+//      (stream-ordered allocations from a memory pool, uploaded on a side
+//      stream); they join the tables at the next step.
 // Kernels and arithmetic are those of a single-job set, so each job's
 // result equals its own plain run bit for bit.
 #include <algorithm>
@@ -41,6 +43,8 @@ struct SJob {
     void *mem = nullptr;
     int slot = -1;
     DomDev dom{};
+    TimeCtl t0{};        // initial time state, written at the next rebuild
+    bool fresh = false;  // admitted after the last graph launch
     double t_submit = 0, t_admit = 0;
 };
 
@@ -88,6 +92,7 @@ struct lulesh_server {
     size_t blocks_cap = 0;
     int2 *cp_b = nullptr, *node_b = nullptr, *elem_b = nullptr;
     int n_cp = 0, n_node = 0, n_elem = 0;
+    int n_table = 0;  // domains in the launched tables
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     bool dirty = true;
@@ -150,6 +155,15 @@ static int rebuild(lulesh_server *s)
     if (!hd.empty())
         SCHECK(cudaMemcpyAsync(s->ddoms, hd.data(), sizeof(DomDev) * hd.size(),
                                cudaMemcpyHostToDevice, s->stream));
+    // jobs admitted since the last launch get their time state now, on the
+    // compute stream after the previous step: no launched cycle sees it
+    SCHECK(cudaStreamSynchronize(s->upload));
+    for (auto &j : s->active)
+        if (j->fresh) {
+            SCHECK(cudaMemcpyAsync(s->dtc + j->slot, &j->t0, sizeof(TimeCtl),
+                                   cudaMemcpyHostToDevice, s->stream));
+            j->fresh = false;
+        }
     const size_t need = cb.size() + nb.size() + eb.size();
     if (need > s->blocks_cap) {
         if (s->dblocks) SCHECK(cudaFreeAsync(s->dblocks, s->stream));
@@ -175,11 +189,12 @@ static int rebuild(lulesh_server *s)
     // the host vectors above are pageable: the copies complete before return
     SCHECK(cudaStreamSynchronize(s->stream));
 
-    if (s->exec) cudaGraphExecDestroy(s->exec);
-    if (s->graph) cudaGraphDestroy(s->graph);
-    s->exec = nullptr;
-    s->graph = nullptr;
-    if (!hd.empty()) {
+    if (hd.empty()) {
+        if (s->exec) cudaGraphExecDestroy(s->exec);
+        if (s->graph) cudaGraphDestroy(s->graph);
+        s->exec = nullptr;
+        s->graph = nullptr;
+    } else {
         SCHECK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
         launch_time_increment(s->dtc, s->cfg.max_jobs, s->P, s->stream);
 #if LULESH_FORCE_CP
@@ -192,9 +207,21 @@ static int rebuild(lulesh_server *s)
         launch_eos(s->args(s->elem_b), s->n_elem, s->P, s->stream);
         cudaGraph_t g = nullptr;
         SCHECK(cudaStreamEndCapture(s->stream, &g));
+        // same five kernels every time, only their grids and tables change:
+        // update the executable graph in place, instantiate only if that fails
+        if (s->exec) {
+            cudaGraphExecUpdateResultInfo info{};
+            if (cudaGraphExecUpdate(s->exec, g, &info) != cudaSuccess) {
+                (void)cudaGetLastError();
+                cudaGraphExecDestroy(s->exec);
+                s->exec = nullptr;
+            }
+        }
+        if (s->graph) cudaGraphDestroy(s->graph);
         s->graph = g;
-        SCHECK(cudaGraphInstantiate(&s->exec, g, 0));
+        if (!s->exec) SCHECK(cudaGraphInstantiate(&s->exec, g, 0));
     }
+    s->n_table = (int)hd.size();
     s->dirty = false;
     return LULESH_OK;
 }
@@ -321,7 +348,7 @@ int lulesh_server_step(lulesh_server *s, int *n_active, int *n_queued)
         std::vector<std::shared_ptr<SJob>> keep;
         for (auto &j : s->active) {
             const TimeCtl &T = s->htc[j->slot];
-            if (!T.done) {
+            if (j->fresh || !T.done) {  // a fresh job's record was not read back
                 keep.push_back(j);
                 continue;
             }
@@ -343,7 +370,28 @@ int lulesh_server_step(lulesh_server *s, int *n_active, int *n_queued)
         }
         s->active.swap(keep);
     }
-    // 2. admit in arrival order
+    // 2. resident set changed: new tables and graph
+    if (s->dirty) {
+        int st = rebuild(s);
+        if (st != LULESH_OK) return st;
+    }
+    // 3. advance every resident job
+    if (s->n_table > 0) {
+        for (int c = 0; c < s->cfg.cycles_per_step; ++c)
+            SCHECK(cudaGraphLaunch(s->exec, s->stream));
+        const int n = s->n_table;
+        k_gather_origin<<<(n + 127) / 128, 128, 0, s->stream>>>(s->ddoms, n, s->denergy);
+        SCHECK(cudaGetLastError());
+        SCHECK(cudaMemcpyAsync(s->htc, s->dtc, sizeof(TimeCtl) * s->cfg.max_jobs,
+                               cudaMemcpyDeviceToHost, s->stream));
+        SCHECK(cudaMemcpyAsync(s->henergy, s->denergy, sizeof(double) * s->cfg.max_jobs,
+                               cudaMemcpyDeviceToHost, s->stream));
+        SCHECK(cudaEventRecord(s->step_done, s->stream));
+        s->in_flight = true;
+    }
+    // 4. admit in arrival order while the step runs: the uploads (side
+    //    stream, host-blocking pageable copies) overlap the GPU's cycles;
+    //    the jobs join the tables, and get their time state, at the next step
     while (!s->pending.empty()) {
         auto &j = s->pending.front();
         if (!j->ready.load(std::memory_order_acquire)) break;
@@ -357,37 +405,18 @@ int lulesh_server_step(lulesh_server *s, int *n_active, int *n_queued)
             cudaFreeAsync(mem, s->upload);
             return st;
         }
-        TimeCtl T0 = initial_timectl(j->host->deltatime, j->job.its);
-        SCHECK(cudaMemcpyAsync(s->dtc + slot, &T0, sizeof T0, cudaMemcpyHostToDevice, s->upload));
+        j->t0 = initial_timectl(j->host->deltatime, j->job.its);
         SCHECK(cudaStreamSynchronize(s->upload));
         j->host.reset();
         j->mem = mem;
         j->slot = slot;
+        j->fresh = true;
         j->t_admit = mono_now();
         s->free_slots.pop_back();
         s->used_bytes += j->bytes;
         s->active.push_back(j);
         s->pending.pop_front();
         s->dirty = true;
-    }
-    // 3. resident set changed: new tables and graph
-    if (s->dirty) {
-        int st = rebuild(s);
-        if (st != LULESH_OK) return st;
-    }
-    // 4. advance
-    if (!s->active.empty()) {
-        for (int c = 0; c < s->cfg.cycles_per_step; ++c)
-            SCHECK(cudaGraphLaunch(s->exec, s->stream));
-        const int n = (int)s->active.size();
-        k_gather_origin<<<(n + 127) / 128, 128, 0, s->stream>>>(s->ddoms, n, s->denergy);
-        SCHECK(cudaGetLastError());
-        SCHECK(cudaMemcpyAsync(s->htc, s->dtc, sizeof(TimeCtl) * s->cfg.max_jobs,
-                               cudaMemcpyDeviceToHost, s->stream));
-        SCHECK(cudaMemcpyAsync(s->henergy, s->denergy, sizeof(double) * s->cfg.max_jobs,
-                               cudaMemcpyDeviceToHost, s->stream));
-        SCHECK(cudaEventRecord(s->step_done, s->stream));
-        s->in_flight = true;
     }
     if (n_active) *n_active = (int)s->active.size();
     if (n_queued) *n_queued = (int)s->pending.size();

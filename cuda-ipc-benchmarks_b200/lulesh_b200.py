@@ -61,7 +61,8 @@ EXPORTED = [
     "lulesh_server_create", "lulesh_server_destroy", "lulesh_server_submit",
     "lulesh_server_step", "lulesh_server_poll", "lulesh_server_clock",
     "lulesh_set_graph_cycles", "lulesh_get_tuning", "lulesh_set_tuning",
-    "lulesh_autotune",
+    "lulesh_autotune", "lulesh_checkpoint_bytes", "lulesh_checkpoint_save",
+    "lulesh_checkpoint_load",
 ]
 
 
@@ -173,6 +174,9 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "lulesh_set_tuning": (ip, [vp, ctypes.POINTER(Tuning)]),
         "lulesh_autotune": (ip, [vp, ip, ip, ctypes.POINTER(Tuning), ctypes.POINTER(TuneTrial),
                                  ip, ctypes.POINTER(ip)]),
+        "lulesh_checkpoint_bytes": (ctypes.c_size_t, [vp]),
+        "lulesh_checkpoint_save": (ip, [vp, vp, ctypes.c_size_t]),
+        "lulesh_checkpoint_load": (ip, [vp, vp, ctypes.c_size_t]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -294,6 +298,19 @@ class LuleshSet:
         return {"best": best.as_dict(),
                 "trials": [dict(trials[i].tuning.as_dict(), ms_per_cycle=trials[i].ms_per_cycle)
                            for i in range(n.value)]}
+
+    def checkpoint(self) -> bytes:
+        """The set's whole state (header + device arrays + time state)."""
+        n = int(self.lib.lulesh_checkpoint_bytes(self.h))
+        buf = ctypes.create_string_buffer(n)
+        _check(self.lib, self.lib.lulesh_checkpoint_save(self.h, buf, n), "lulesh_checkpoint_save")
+        return buf.raw
+
+    def restore(self, ckpt: bytes) -> None:
+        """Load a checkpoint taken from a set with the same jobs, tp and flags."""
+        buf = ctypes.create_string_buffer(ckpt, len(ckpt))
+        _check(self.lib, self.lib.lulesh_checkpoint_load(self.h, buf, len(ckpt)),
+               "lulesh_checkpoint_load")
 
     def profile_phases(self, ncycles: int) -> dict:
         """Average ms per phase over `ncycles` separately launched cycles."""

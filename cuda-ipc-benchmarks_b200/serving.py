@@ -8,6 +8,12 @@ plain   the same stream, first come first served, one job at a time through
 Job latency = completion time - arrival time (wall clock); throughput =
 sum of the jobs' zone-cycles / (last completion - first arrival).  Both runs
 check every job's Final Origin Energy against the other's.
+
+At lambda = 50/s the served form keeps up with arrivals, so its throughput
+over the makespan is bounded by the offered load.  Capacity is measured
+separately: the served form replays the same jobs all queued at t = 0
+(`saturated`), and the plain form's capacity is its zone-cycles over the
+sum of its per-job service times (run time without queueing).
 """
 from __future__ import annotations
 
@@ -34,6 +40,11 @@ def make_stream(n_jobs: int = 2000, lam: float = 50.0, seed: int = 0,
              "cost": 1, "its": int(its[i])} for i in range(n_jobs)]
 
 
+def saturated(stream: list[dict]) -> list[dict]:
+    """The same jobs, all arriving at t = 0."""
+    return [dict(j, arrive=0.0) for j in stream]
+
+
 def _spec(j):
     return L.JobSpec(j["nx"], j["numReg"], j["balance"], j["cost"], j["its"])
 
@@ -47,7 +58,7 @@ def _summary(stream, lat, done_at, cycles, t0):
             "makespan_s": makespan, "zone_cycles": zc, "zone_cycles_per_s": zc / makespan}
 
 
-def run_served(stream, hbm_cap_bytes=150 * 10**9, max_jobs=512, cycles_per_step=8,
+def run_served(stream, hbm_cap_bytes=150 * 10**9, max_jobs=512, cycles_per_step=64,
                prepare_threads=8, device=0):
     srv = L.Server(hbm_cap_bytes=hbm_cap_bytes, max_jobs=max_jobs,
                    cycles_per_step=cycles_per_step, prepare_threads=prepare_threads,
@@ -82,10 +93,12 @@ def run_plain(stream, device=0):
     n = len(stream)
     t0 = time.perf_counter()
     lat, done_at, cycles, energy = [], [], [], []
+    service = 0.0
     for j in stream:
         wait = j["arrive"] - (time.perf_counter() - t0)
         if wait > 0:
             time.sleep(wait)
+        ts = time.perf_counter()
         with L.LuleshSet(nx=j["nx"], numReg=j["numReg"], balance=j["balance"], cost=j["cost"],
                          its=j["its"], device=device) as s:
             st = s.run()
@@ -94,15 +107,22 @@ def run_plain(stream, device=0):
             if st != L.OK:
                 raise RuntimeError(f"plain job failed with status {st}")
         t = time.perf_counter()
+        service += t - ts
         done_at.append(t)
         lat.append(t - (t0 + j["arrive"]))
-    return _summary(stream, lat, done_at, cycles, t0), energy
+    out = _summary(stream, lat, done_at, cycles, t0)
+    out["service_s"] = service
+    out["capacity_zone_cycles_per_s"] = out["zone_cycles"] / service
+    return out, energy
 
 
 def compare(stream, **kw) -> dict:
     served, e_served = run_served(stream, **kw)
+    sat, e_sat = run_served(saturated(stream), **kw)
     plain, e_plain = run_plain(stream, device=kw.get("device", 0))
     mism = sum(1 for a, b in zip(e_served, e_plain) if a != b)
-    return {"served": served, "plain": plain,
+    mism += sum(1 for a, b in zip(e_sat, e_plain) if a != b)
+    return {"served": served, "served_saturated": sat, "plain": plain,
             "throughput_ratio": served["zone_cycles_per_s"] / plain["zone_cycles_per_s"],
+            "capacity_ratio": sat["zone_cycles_per_s"] / plain["capacity_zone_cycles_per_s"],
             "energy_mismatches": mism}

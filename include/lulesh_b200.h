@@ -150,6 +150,18 @@ int lulesh_step(lulesh_set *set, int ncycles);
  * one-cycle graph, so a whole batch run can be a single graph launch. */
 int lulesh_set_graph_cycles(lulesh_set *set, int k);
 
+/* Checkpoint of a set's whole state: every device array of every domain
+ * and the time state of every job, behind a header that identifies the
+ * set's jobs, subdomain count and flags.  No reference counterpart (the
+ * reference has no restart path).  A checkpoint loads only into a set
+ * created with the same jobs, tp and flags (else LULESH_INVALID_ARG);
+ * stepping on from a loaded checkpoint gives the same results, bit for
+ * bit, as stepping on from where it was saved.  Both calls synchronise the
+ * set's stream. */
+size_t lulesh_checkpoint_bytes(const lulesh_set *set);
+int lulesh_checkpoint_save(lulesh_set *set, void *host_buf, size_t bytes);
+int lulesh_checkpoint_load(lulesh_set *set, const void *host_buf, size_t bytes);
+
 /* Launch shapes of a set.  No reference counterpart (the reference launches
  * fixed 64/128-thread blocks per kernel); results do not depend on them. */
 typedef struct lulesh_tuning {
