@@ -150,8 +150,20 @@ int upload_domain(const HostDomain &h, int tc, long comm_doubles, bool mixed, Ca
     DCHECK(cudaMemsetAsync(D.fy_elem, 0, 8 * 8 * z.Ep, st));
     DCHECK(cudaMemsetAsync(D.fz_elem, 0, 8 * 8 * z.Ep, st));
     if (z.comm) DCHECK(cudaMemsetAsync(D.commRecv, 0, 8 * z.comm, st));
-    std::vector<double> ones(E, 1.0);
     int su;
+    if (h.device_geometry) {
+        // single domain: geometry on the device, regions from the host
+        if ((su = setup_geometry_on_device(D, h.einit, st)) != LULESH_OK) return su;
+        const std::vector<int> *rv[] = {&h.regNumList, &h.regElemlist, &h.regCSR,
+                                        &h.regReps,    &h.regSorted,   &h.eosOrder};
+        int *rp[] = {D.regNumList, D.regElemlist, D.regCSR, D.regReps, D.regSorted, D.eosOrder};
+        for (size_t k = 0; k < sizeof(rp) / sizeof(rp[0]); ++k)
+            if ((su = upload(rp[k], *rv[k], st)) != LULESH_OK) return su;
+        DCHECK(cudaStreamSynchronize(st));
+        *out = D;
+        return LULESH_OK;
+    }
+    std::vector<double> ones(E, 1.0);
     if ((su = upload(D.v, ones, st)) != LULESH_OK) return su;
     if ((su = upload(D.e, h.e, st)) != LULESH_OK) return su;
     if ((su = upload(D.volo, h.volo, st)) != LULESH_OK) return su;

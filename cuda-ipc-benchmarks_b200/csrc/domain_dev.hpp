@@ -41,6 +41,11 @@ struct Carver {
 int upload_domain(const HostDomain &h, int tc, long comm_doubles, bool mixed, Carver &cv,
                   cudaStream_t st, DomDev *D, CornerF32 *c32);
 
+// Write the geometry and connectivity arrays of single domain D (tp = 1) on
+// the device (setup.cu), with the values build_domain computes on the
+// host; e[0] = einit.  Asynchronous on `st`.
+int setup_geometry_on_device(const DomDev &D, double einit, cudaStream_t st);
+
 // The time state of a job before its first cycle (lulesh.cu:1120-1132).
 TimeCtl initial_timectl(double deltatime, int its_cap);
 

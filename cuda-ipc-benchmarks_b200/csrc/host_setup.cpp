@@ -467,4 +467,38 @@ void build_domain(HostDomain &d, int nx, int tp, int col, int row, int plane,
     build_regions(d, numReg, balance);
 }
 
+void build_domain_light(HostDomain &d, int nx, int numReg, int balance, int cost)
+{
+    const int en = nx + 1;
+    d.nx = nx;
+    d.en = en;
+    d.tp = 1;
+    d.col = d.row = d.plane = d.rank = 0;
+    d.cost = cost;
+    d.numElem = nx * nx * nx;
+    d.Ep = ((d.numElem + 31) / 32) * 32;
+    d.numNode = en * en * en;
+    d.rowMin = d.rowMax = d.colMin = d.colMax = d.planeMin = d.planeMax = 0;
+    d.allElem = d.numElem + 6 * nx * nx;
+    d.numSymmX = d.numSymmY = d.numSymmZ = en * en;
+    for (int f = 0; f < 6; ++f) d.ghost[f] = -1;
+    d.device_geometry = true;
+    // volume of element 0 for the initial dt (the corner at the origin)
+    double xl[8], yl[8], zl[8];
+    const int dx[8] = {0, 1, 1, 0, 0, 1, 1, 0};
+    const int dy[8] = {0, 0, 1, 1, 0, 0, 1, 1};
+    const int dz[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+    for (int k = 0; k < 8; ++k) {
+        xl[k] = lattice(dx[k], nx);
+        yl[k] = lattice(dy[k], nx);
+        zl[k] = lattice(dz[k], nx);
+    }
+    const double volo0 = elem_volume_host(xl, yl, zl);
+    const double ebase = 3.948746e+7;
+    double scale = nx / 45.0;
+    d.einit = ebase * scale * scale * scale;
+    d.deltatime = (.5 * cbrt(volo0)) / sqrt(2 * d.einit);
+    build_regions(d, numReg, balance);
+}
+
 }  // namespace lulesh

@@ -47,6 +47,9 @@ struct HostDomain {
     std::vector<double> x, y, z, volo, elemMass, nodalMass, e;
     double einit = 0.0;
     double deltatime = 0.0;  // initial dt of this domain, lulesh.cu:1205
+    // geometry and connectivity left to the device (build_domain_light):
+    // the vectors from nodelist to nodalMass above are empty
+    bool device_geometry = false;
 };
 
 // Reference parameter block, lulesh.cu:1125-1158.
@@ -59,6 +62,13 @@ Params default_params();
 // contribute (what each rank holds before the init-time CommSBN).
 void build_domain(HostDomain &d, int nx, int tp, int col, int row, int plane,
                   int rank, int numReg, int balance, int cost, bool global_mass);
+
+// A single (tp = 1) domain with only what must come from the host: the
+// scalars, the energy deposit and initial dt, and the region sets drawn
+// from glibc rand (with the EOS order).  The geometry and connectivity are
+// generated on the device (setup.cu) with the same values build_domain
+// computes.
+void build_domain_light(HostDomain &d, int nx, int numReg, int balance, int cost);
 
 // CalcElemVolume (lulesh.cu:221-307), host copy used at setup.
 double elem_volume_host(const double *x, const double *y, const double *z);

@@ -1,7 +1,8 @@
 // server.cu -- continuous batching of sedov jobs on one GPU.
 //
-// Submitted jobs are meshed on host worker threads (build_domain, the
-// NewDomain restatement).  lulesh_server_step then
+// Submitted jobs get their region sets (glibc rand) on host worker threads
+// (build_domain_light); their geometry is generated on the device at
+// admission (setup.cu).  lulesh_server_step then
 //   1. waits for the previous step, reads every slot's time control and
 //      origin energy (one gather kernel + two small copies issued at the end
 //      of that step) and retires finished jobs, freeing their memory;
@@ -128,8 +129,7 @@ static void prep_worker(lulesh_server *s)
             s->prep_q.pop_front();
         }
         auto h = std::make_unique<HostDomain>();
-        build_domain(*h, j->job.nx, 1, 0, 0, 0, 0, j->job.numReg, j->job.balance, j->job.cost,
-                     false);
+        build_domain_light(*h, j->job.nx, j->job.numReg, j->job.balance, j->job.cost);
         j->host = std::move(h);
         j->ready.store(true, std::memory_order_release);
     }

@@ -135,8 +135,11 @@ static int create_common(lulesh_set *s, const std::vector<DomPlace> &place, int 
         const DomPlace &pl = place[d];
         const lulesh_job &j = s->jobs[pl.job];
         HostDomain h;
-        build_domain(h, j.nx, pl.tp, pl.col, pl.row, pl.plane, pl.rank, j.numReg, j.balance,
-                     j.cost, /*global_mass=*/pl.tp > 1);
+        if (pl.tp == 1 && !(s->flags & LULESH_FLAG_HOST_SETUP))
+            build_domain_light(h, j.nx, j.numReg, j.balance, j.cost);
+        else
+            build_domain(h, j.nx, pl.tp, pl.col, pl.row, pl.plane, pl.rank, j.numReg, j.balance,
+                         j.cost, /*global_mass=*/pl.tp > 1);
         DomDev D{};
         int su = upload_domain(h, pl.job, commd[d], mixed, cv, s->stream, &D, &hc32[d]);
         if (su != LULESH_OK) return su;

@@ -29,6 +29,7 @@ NO_DEVICE = -8
 FLAG_MATERIALIZE = 0x1
 FLAG_COMM_STAGED = 0x2
 FLAG_MIXED = 0x4
+FLAG_HOST_SETUP = 0x8
 
 MSG_COMM_SBN = 1024
 MSG_SYNC_POS_VEL = 2048

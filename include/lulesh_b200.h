@@ -62,6 +62,11 @@ enum lulesh_status {
                                        kinematics arithmetic, compensated
                                        FP32 corner-force sums, FP64 EOS,
                                        node integration and dt              */
+#define LULESH_FLAG_HOST_SETUP 0x8  /* build single-domain geometry and
+                                       connectivity on the host and copy it
+                                       (as NewDomain does) instead of
+                                       generating it on the device; the
+                                       values are the same either way      */
 
 /* One sedov job: the reference command line -s -r -b -c -i
  * (LULESH/omp_4.0/lulesh-util.cc:60-173; defaults 30/11/1/1). */

@@ -159,3 +159,34 @@ def test_global_nodal_mass_equals_undecomposed(host):
         sub = _field(host, "nodalMass", nx, tp, c, w, p, r, gm=1).reshape(nx + 1, nx + 1, nx + 1)
         ref = full[p * nx:(p + 1) * nx + 1, w * nx:(w + 1) * nx + 1, c * nx:(c + 1) * nx + 1]
         assert np.array_equal(sub, ref), r
+
+
+@pytest.mark.parametrize("nx", [1, 2, 3, 7, 12])
+def test_closed_form_corner_csr(host, nx):
+    """The closed forms the device setup kernel uses for nodeElemStart,
+    nodeElemCount and nodeElemCornerList (setup.cu) reproduce the host
+    builder's prefix-sum CSR (lulesh.cu:1054-1106)."""
+    en, Ep = nx + 1, ((nx ** 3 + 31) // 32) * 32
+    start = _field(host, "nodeElemStart", nx)
+    count = _field(host, "nodeElemCount", nx)
+    corners = _field(host, "nodeElemCornerList", nx)
+
+    def adj(p):
+        return (p > 0) + (p < nx)
+
+    def below(k):
+        return 0 if k == 0 else 2 * k - 1
+    A = 2 * nx
+    got = np.full_like(corners, -1)
+    for n in range(en ** 3):
+        px, t = n % en, n // en
+        py, pz = t % en, t // en
+        s = below(pz) * A * A + adj(pz) * below(py) * A + adj(pz) * adj(py) * below(px)
+        assert s == start[n] and adj(px) * adj(py) * adj(pz) == count[n]
+        r = 0
+        for j in range(8):
+            ex, ey, ez = px - ((0x66 >> j) & 1), py - ((0xCC >> j) & 1), pz - ((0xF0 >> j) & 1)
+            if 0 <= ex < nx and 0 <= ey < nx and 0 <= ez < nx:
+                got[s + r] = Ep * j + (ez * nx + ey) * nx + ex
+                r += 1
+    assert np.array_equal(got, corners)
