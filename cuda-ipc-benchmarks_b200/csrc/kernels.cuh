@@ -12,7 +12,8 @@ constexpr int kNodeBlock = 128;  // threads per block, node kernels
 
 // Resident blocks per SM asked of the compiler (the register budget of the
 // element kernels), chosen by measurement on B200 at -s 100: kinematics 3
-// (<= 170 registers, 118 -> 92 us), EOS 8 (64 registers, 134 -> 98 us).
+// (<= 170 registers, 118 -> 92 us), EOS 12 (40 registers with small spills;
+// 134 us unbounded, 97 us at 8 blocks, 86 us at 12, 88 us at 16).
 #ifndef LULESH_FORCE_MINB
 #define LULESH_FORCE_MINB 1
 #endif
@@ -23,7 +24,7 @@ constexpr int kNodeBlock = 128;  // threads per block, node kernels
 #define LULESH_KIN_MINB 3
 #endif
 #ifndef LULESH_EOS_MINB
-#define LULESH_EOS_MINB 8
+#define LULESH_EOS_MINB 12
 #endif
 constexpr int kForceCpMinBlocks = LULESH_FORCECP_MINB;
 constexpr int kForceMinBlocks = LULESH_FORCE_MINB;
