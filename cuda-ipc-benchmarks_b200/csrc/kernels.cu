@@ -214,7 +214,7 @@ __device__ __forceinline__ void gather_corners(const DomDev *doms, const DomDev 
 //         writing fx/fy/fz (the partial sums the reference exchanges).
 // MODE 2: the node update from fx/fy/fz (after CommSBN added neighbours).
 template <int MODE, int BS>
-__global__ void __launch_bounds__(BS) k_nodal(SetArgs a, Params P)
+__global__ void __launch_bounds__(BS, min_blocks(kNodalMinBlocks, BS)) k_nodal(SetArgs a, Params P)
 {
     const int2 blk = a.blocks[blockIdx.x];
     const DomDev &D = a.doms[blk.x];
