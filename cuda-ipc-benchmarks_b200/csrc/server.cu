@@ -313,7 +313,7 @@ int lulesh_server_destroy(lulesh_server *s)
 
 int lulesh_server_submit(lulesh_server *s, const lulesh_job *job, long long *id)
 {
-    if (!s || !job || job->nx < 1 || job->nx > 1024 || job->numReg < 1 || job->balance < 0 ||
+    if (!s || !job || job->nx < 1 || job->nx > LULESH_MAX_NX || job->numReg < 1 || job->balance < 0 ||
         job->cost < 0) {
         set_error("lulesh_server_submit: bad job");
         return LULESH_INVALID_ARG;

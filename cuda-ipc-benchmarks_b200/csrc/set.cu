@@ -35,9 +35,15 @@ int cuda_status(cudaError_t e, const char *what)
 
 static int validate_job(const lulesh_job &j)
 {
-    if (j.nx < 1 || j.nx > 1024 || j.numReg < 1 || j.numReg > 1000 || j.balance < 0 ||
-        j.balance > 30 || j.cost < 0 || j.cost > 1000) {
-        set_error("invalid job parameters (nx in [1,1024], numReg >= 1, balance/cost >= 0)");
+    if (j.nx > LULESH_MAX_NX) {
+        set_error("nx above LULESH_MAX_NX (645): its 32-bit corner indices would overflow; "
+                  "run the mesh as tp^3 subdomains");
+        return LULESH_INVALID_ARG;
+    }
+    if (j.nx < 1 || j.numReg < 1 || j.numReg > 1000 || j.balance < 0 || j.balance > 30 ||
+        j.cost < 0 || j.cost > 1000) {
+        set_error("invalid job parameters (nx >= 1, numReg in [1,1000], balance in [0,30], "
+                  "cost in [0,1000])");
         return LULESH_INVALID_ARG;
     }
     return LULESH_OK;

@@ -31,6 +31,8 @@ FLAG_COMM_STAGED = 0x2
 FLAG_MIXED = 0x4
 FLAG_HOST_SETUP = 0x8
 
+MAX_NX = 645  # LULESH_MAX_NX
+
 MSG_COMM_SBN = 1024
 MSG_SYNC_POS_VEL = 2048
 MSG_MONOQ = 3072

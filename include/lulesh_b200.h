@@ -68,10 +68,18 @@ enum lulesh_status {
                                        generating it on the device; the
                                        values are the same either way      */
 
+/* Largest edge of one domain.  Corner forces are indexed
+ * elem + padded_numElem * corner in 32-bit integers, as in the reference
+ * (Index_t = int32, lulesh.h:32-33, lulesh.cu:2242); at nx = 646 that index
+ * passes 2^31 - 1 while the mesh (~157 GB) would still fit in HBM.  Larger
+ * jobs are rejected with LULESH_INVALID_ARG; a larger global mesh runs as
+ * tp^3 subdomains of at most this edge. */
+#define LULESH_MAX_NX 645
+
 /* One sedov job: the reference command line -s -r -b -c -i
  * (LULESH/omp_4.0/lulesh-util.cc:60-173; defaults 30/11/1/1). */
 typedef struct lulesh_job {
-    int nx;      /* -s: elements per edge of each (sub)domain, >= 1       */
+    int nx;      /* -s: elements per edge of each (sub)domain, 1..645      */
     int numReg;  /* -r: regions (cost model only), >= 1                  */
     int balance; /* -b                                                    */
     int cost;    /* -c                                                    */

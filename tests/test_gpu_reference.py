@@ -65,3 +65,22 @@ def test_config2_subdomains_full_size(lulesh):
     ref = CUDA_REF.get("-s 100 -i 500")
     if ref:
         assert abs(e1 - ref["energy"]) <= 1e-9 * abs(ref["energy"])
+
+
+def test_largest_domain(lulesh):
+    """nx = LULESH_MAX_NX (645): 268 million elements, ~152 GB on the device.
+    The largest 32-bit corner index is in range and a few cycles run clean,
+    with the plane-0 energy as symmetric as at small sizes."""
+    try:
+        s = lulesh.LuleshSet(nx=lulesh.MAX_NX, its=3)
+    except lulesh.LuleshError as e:
+        if e.status == lulesh.OOM:
+            pytest.skip("not enough free device memory for nx = 645")
+        raise
+    with s:
+        assert s.run() == lulesh.OK
+        st = s.state()
+        assert st["cycle"] == 3 and st["status"] == 0
+        e0 = s.origin_energy()
+        assert e0 > 0 and e0 == e0
+        assert s.symmetry()[2] < 1e-10

@@ -44,3 +44,16 @@ def test_footprint_model_without_device(lulesh):
     assert 400 * 10**6 < one < 800 * 10**6
     two = lulesh.footprint_bytes([lulesh.JobSpec(50)], tp=2)
     assert two > one * 0.9  # 8 subdomains of 50^3 plus comm buffers
+
+
+def test_oversize_job_rejected_before_touching_a_device(lulesh):
+    """nx above LULESH_MAX_NX (645) would overflow the 32-bit corner index
+    elem + padded_numElem * corner; lulesh_create refuses it up front."""
+    lib = lulesh.load_library()
+    h = ctypes.c_void_p()
+    for nx in (646, 1000):
+        job = lulesh.JobSpec(nx).c()
+        st = lib.lulesh_create(ctypes.byref(job), 1, 0, -1, ctypes.byref(h))
+        assert st == lulesh.INVALID_ARG and not h.value
+        assert b"645" in lib.lulesh_last_error()
+    assert lulesh.MAX_NX == 645
