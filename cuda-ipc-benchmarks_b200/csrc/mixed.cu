@@ -21,6 +21,16 @@
 
 namespace lulesh {
 
+// Resident blocks per SM asked of the compiler for the mixed kernels:
+// 5 (96 registers) measured best on B200 at -s 100 (force 82 -> 78 us,
+// kinematics 70 -> 66 us against the unbounded build)
+#ifndef LULESH_MIXED_FORCE_MINB
+#define LULESH_MIXED_FORCE_MINB 5
+#endif
+#ifndef LULESH_MIXED_KIN_MINB
+#define LULESH_MIXED_KIN_MINB 5
+#endif
+
 __device__ __forceinline__ void elem_nodes_m(const DomDev &D, int el, int n[8])
 {
     const int nx = D.nx, en = D.en;
@@ -37,8 +47,8 @@ __device__ __forceinline__ void elem_nodes_m(const DomDev &D, int el, int n[8])
 }
 
 template <bool HG>
-__global__ void __launch_bounds__(kElemBlock) k_force_mixed(SetArgs a, Params P,
-                                                            const CornerF32 *cfs)
+__global__ void __launch_bounds__(kElemBlock, LULESH_MIXED_FORCE_MINB)
+    k_force_mixed(SetArgs a, Params P, const CornerF32 *cfs)
 {
     const int2 blk = a.blocks[blockIdx.x];
     const DomDev &D = a.doms[blk.x];
@@ -50,6 +60,17 @@ __global__ void __launch_bounds__(kElemBlock) k_force_mixed(SetArgs a, Params P,
 
     int n[8];
     elem_nodes_m(D, elem, n);
+    // all node gathers first: the velocities arrive while the coordinate
+    // arithmetic runs
+    float vx[8], vy[8], vz[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        if (HG) {
+            vx[i] = (float)D.xd[n[i]];
+            vy[i] = (float)D.yd[n[i]];
+            vz[i] = (float)D.zd[n[i]];
+        }
+    }
     const double x0 = D.x[n[0]], y0 = D.y[n[0]], z0 = D.z[n[0]];
     float xn[8], yn[8], zn[8];
 #pragma unroll
@@ -82,23 +103,17 @@ __global__ void __launch_bounds__(kElemBlock) k_force_mixed(SetArgs a, Params P,
         hgfz[i] = -(sigxx * B[2][i]);
     }
     if (HG) {
-        float vel[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) vel[i] = (float)D.xd[n[i]];
-        fb_hourglass_component(vel, hourgam, coefficient, hgfx);
-#pragma unroll
-        for (int i = 0; i < 8; ++i) vel[i] = (float)D.yd[n[i]];
-        fb_hourglass_component(vel, hourgam, coefficient, hgfy);
-#pragma unroll
-        for (int i = 0; i < 8; ++i) vel[i] = (float)D.zd[n[i]];
-        fb_hourglass_component(vel, hourgam, coefficient, hgfz);
+        fb_hourglass_component(vx, hourgam, coefficient, hgfx);
+        fb_hourglass_component(vy, hourgam, coefficient, hgfy);
+        fb_hourglass_component(vz, hourgam, coefficient, hgfz);
     }
+    // written once, read once by the nodal gather: evict-first
     const int Ep = D.Ep;
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-        cf.fx[elem + Ep * k] = hgfx[k];
-        cf.fy[elem + Ep * k] = hgfy[k];
-        cf.fz[elem + Ep * k] = hgfz[k];
+        __stcs(cf.fx + elem + Ep * k, hgfx[k]);
+        __stcs(cf.fy + elem + Ep * k, hgfy[k]);
+        __stcs(cf.fz + elem + Ep * k, hgfz[k]);
     }
 }
 
@@ -122,8 +137,8 @@ __device__ __forceinline__ void comp_add(float &s, float &c, float v)
     s = t;
 }
 
-__global__ void __launch_bounds__(kNodeBlock) k_nodal_mixed(SetArgs a, Params P,
-                                                            const CornerF32 *cfs)
+__global__ void __launch_bounds__(kNodeBlock, min_blocks(kNodalMinBlocks, kNodeBlock))
+    k_nodal_mixed(SetArgs a, Params P, const CornerF32 *cfs)
 {
     const int2 blk = a.blocks[blockIdx.x];
     const DomDev &D = a.doms[blk.x];
@@ -143,9 +158,9 @@ __global__ void __launch_bounds__(kNodeBlock) k_nodal_mixed(SetArgs a, Params P,
         if ((unsigned)ex < (unsigned)nx && (unsigned)ey < (unsigned)nx &&
             (unsigned)ez < (unsigned)nx) {
             const int idx = j * D.Ep + (ez * nx + ey) * nx + ex;
-            comp_add(sx, cx, cf.fx[idx]);
-            comp_add(sy, cy, cf.fy[idx]);
-            comp_add(sz, cz, cf.fz[idx]);
+            comp_add(sx, cx, __ldcs(cf.fx + idx));
+            comp_add(sy, cy, __ldcs(cf.fy + idx));
+            comp_add(sz, cz, __ldcs(cf.fz + idx));
         }
     }
     const double fx = (double)sx + (double)cx;
@@ -185,7 +200,8 @@ void launch_nodal_mixed(const SetArgs &a, int nblocks, Params P, const CornerF32
     k_nodal_mixed<<<nblocks, kNodeBlock, 0, s>>>(a, P, cf);
 }
 
-__global__ void __launch_bounds__(kElemBlock) k_kinematics_mixed(SetArgs a, Params P)
+__global__ void __launch_bounds__(kElemBlock, LULESH_MIXED_KIN_MINB)
+    k_kinematics_mixed(SetArgs a, Params P)
 {
     const int2 blk = a.blocks[blockIdx.x];
     const DomDev &D = a.doms[blk.x];
@@ -195,6 +211,14 @@ __global__ void __launch_bounds__(kElemBlock) k_kinematics_mixed(SetArgs a, Para
     if (k >= D.numElem) return;
     int nodes[8];
     elem_nodes_m(D, k, nodes);
+    // velocities gathered first (used after the FP64 volume)
+    float xv[8], yv[8], zv[8];
+#pragma unroll
+    for (int l = 0; l < 8; ++l) {
+        xv[l] = (float)D.xd[nodes[l]];
+        yv[l] = (float)D.yd[nodes[l]];
+        zv[l] = (float)D.zd[nodes[l]];
+    }
     // FP64: volume and relative volume (they feed delv)
     double xd64[8], yd64[8], zd64[8];
 #pragma unroll
@@ -208,15 +232,12 @@ __global__ void __launch_bounds__(kElemBlock) k_kinematics_mixed(SetArgs a, Para
     D.vnew[k] = relativeVolume;
     D.delv[k] = relativeVolume - D.v[k];
     // FP32: everything else, on coordinates relative to corner 0
-    float xl[8], yl[8], zl[8], xv[8], yv[8], zv[8];
+    float xl[8], yl[8], zl[8];
 #pragma unroll
     for (int l = 0; l < 8; ++l) {
         xl[l] = (float)(xd64[l] - xd64[0]);
         yl[l] = (float)(yd64[l] - yd64[0]);
         zl[l] = (float)(zd64[l] - zd64[0]);
-        xv[l] = (float)D.xd[nodes[l]];
-        yv[l] = (float)D.yd[nodes[l]];
-        zv[l] = (float)D.zd[nodes[l]];
     }
     D.arealg[k] = (double)elem_characteristic_length(xl, yl, zl, (float)volume);
     const float dt2 = (float)(0.5 * T.deltatime);
