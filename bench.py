@@ -55,6 +55,27 @@ UNIT = "zone-cycles/s"
 ALG_BYTES = {"force": 152.0, "nodal": 128.0, "kinematics": 176.0, "eos": 204.0}
 ALG_BYTES_STEP = 660.0
 LAUNCHES_PER_CYCLE = 5  # time_increment, force, nodal, kinematics, eos
+# FP64 flops per element of each phase (an FMA counts 2), measured with
+# ncu's smsp__sass_thread_inst_executed_op_{dfma,dadd,dmul}_pred_on counters
+# at -s 64 (profiles/cycle_kernels_s64_full.md); nodal is per node.
+FP64_FLOPS = {"force": 1427.0, "nodal": 50.2, "kinematics": 814.0, "eos": 510.4}
+
+
+def fp64_peak_tflops(dev):
+    """Nominal FP64 (non-tensor) peak of the device: SMs x 64 FMA lanes x 2
+    flops x max SM clock.  No measured FP64 figure exists for this pool."""
+    import torch
+
+    props = torch.cuda.get_device_properties(dev)
+    mhz = 1965.0
+    try:
+        out = subprocess.run(["nvidia-smi", "-i", str(dev), "--query-gpu=clocks.max.sm",
+                              "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                             timeout=20).stdout.strip()
+        mhz = float(out.splitlines()[0])
+    except Exception:
+        pass
+    return props.multi_processor_count * 64 * 2 * mhz * 1e6 / 1e12
 
 
 def measured_peak_gbs():
@@ -252,6 +273,8 @@ def run_ours(a, rank, world, local_rank):
     peak, peak_kind = measured_peak_gbs()
     ach = ALG_BYTES[dom] * ZONES / (phases[dom] / 1e3) / 1e9
     step_ms_sum = sum(phases.values())
+    fp64_peak = fp64_peak_tflops(dev)
+    fp64 = {k: FP64_FLOPS[k] * ZONES / (phases[k] / 1e3) / 1e12 for k in FP64_FLOPS}
     ach_step = ALG_BYTES_STEP * ZONES / (ms / a.steps / 1e3) / 1e9
 
     # end-to-end through the host-driven C-ABI call
@@ -309,6 +332,11 @@ def run_ours(a, rank, world, local_rank):
                      "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind,
                      "alg_bytes_per_zone": ALG_BYTES[dom],
                      "traffic": traffic_per_launch(dom)},
+        "roofline_fp64": {"bound": "fp64", "unit": "TFLOP/s", "peak": fp64_peak,
+                          "peak_kind": "nominal (SMs x 64 FMA x 2 x max SM clock)",
+                          "kernels": {k: {"achieved": v, "frac": v / fp64_peak}
+                                      for k, v in fp64.items()},
+                          "flops_per_element": FP64_FLOPS},
         "roofline_step": {"achieved": ach_step, "frac": ach_step / peak,
                           "alg_bytes_per_zone_cycle": ALG_BYTES_STEP},
         "phases_ms": phases, "phases_sum_ms": step_ms_sum,
