@@ -1,0 +1,64 @@
+"""The lulesh_b200 command line as the reference's harnesses drive and parse
+it: the CUDA form (-s N x ITERS), the harness form (-s N 0 ITERS), the omp
+flags, and the report fields the sbatch scripts read with awk
+(run_lulesh.sbatch:83-85, run_lulesh_lifecycle.sbatch:96-103)."""
+import os
+import re
+import subprocess
+
+import pytest
+
+from conftest import PKG
+
+pytestmark = pytest.mark.gpu
+
+EXE = os.path.join(PKG, "lulesh_b200")
+
+
+def _run(*args, cwd=None):
+    return subprocess.run([EXE, *args], capture_output=True, text=True, timeout=120, cwd=cwd)
+
+
+def _awk(out, pattern, field):
+    """awk '/pattern/{print $field}': every matching line's field."""
+    return [line.split()[field - 1] for line in out.splitlines() if pattern in line]
+
+
+@pytest.mark.parametrize("args", [["-s", "12", "x", "40"], ["-s", "12", "0", "40"],
+                                  ["-s", "12", "-i", "40"]])
+def test_report_fields_parse_like_the_harness(lulesh, args, tmp_path):
+    r = _run(*args, "--no-xyz", cwd=tmp_path) if args[2] == "-i" else _run(*args, cwd=tmp_path)
+    assert r.returncode == 0, r.stdout + r.stderr
+    energy = _awk(r.stdout, "Final Origin Energy", 5)
+    elapsed = _awk(r.stdout, "Elapsed time", 4)
+    fom = _awk(r.stdout, "FOM", 3)
+    assert len(energy) == len(elapsed) == len(fom) == 1, r.stdout
+    assert int(_awk(r.stdout, "Iteration count", 4)[0]) == 40
+    with lulesh.LuleshSet(nx=12, its=40) as s:
+        s.run()
+        e = s.origin_energy()
+    assert energy[0] == f"{e:12.6e}".strip()
+    full = float(re.search(r"Origin energy, 17 digits = (\S+)", r.stdout).group(1))
+    assert full == e
+    float(elapsed[0]), float(fom[0])
+    assert ("xyz.asc" in os.listdir(tmp_path)) == (args[2] != "-i")
+
+
+def test_subdomain_run_prints_lifecycle_lines(tmp_path):
+    r = _run("-s", "8", "-t", "2", "-i", "20", "--no-xyz", cwd=tmp_path)
+    assert r.returncode == 0, r.stdout + r.stderr
+    for name in ("COMM_SETUP", "WIN_ALLOCATE", "PEER_QUERY", "COMM_FREE", "APP_TOTAL"):
+        m = re.search(rf"PHASE_{name}_ms\s+([0-9.]+)", r.stdout)
+        assert m, name
+    assert _awk(r.stdout, "MPI tasks", 4) == ["8"]
+
+
+def test_errors_map_to_reference_exit_codes(tmp_path):
+    # exit(LFileError) with LFileError = -3 (lulesh.h:22-26): status 253
+    assert _run("-u", "mesh.lmesh", cwd=tmp_path).returncode == (-3) & 0xFF
+    r = _run("-s", "8", "--bogus", cwd=tmp_path)
+    assert r.returncode != 0 and "Unknown command line argument" in r.stdout
+    r = _run("-s", "646", "-i", "1", "--no-xyz", cwd=tmp_path)  # above LULESH_MAX_NX
+    assert r.returncode != 0
+    r = _run("-s", "8", "-i", "5", "-q", "--no-xyz", cwd=tmp_path)
+    assert r.returncode == 0 and r.stdout == ""
