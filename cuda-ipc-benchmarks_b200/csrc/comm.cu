@@ -17,6 +17,7 @@
 // one thread per node, so no float atomics are needed.
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <tuple>
 #include <vector>
 
@@ -285,7 +286,17 @@ struct CommCache {
     int2 *surface_blocks = nullptr;
     int n_surface_blocks = 0;
 };
+// One cache per set.  Sets on different host threads may build their
+// tables at the same time, so the map itself is guarded; a set's own entry
+// is used only by the thread driving that set (map nodes do not move).
 static std::map<const lulesh_set *, CommCache> g_comm;
+static std::mutex g_comm_mu;
+
+static CommCache &cache_of(const lulesh_set *s)
+{
+    std::lock_guard<std::mutex> lk(g_comm_mu);
+    return g_comm[s];
+}
 
 // messages that rank `rank` (or every rank, -1) sends
 static int build_msgs(lulesh_set *s, int rank, int xferFields, bool doSend, bool planeOnly,
@@ -341,7 +352,7 @@ static int build_msgs(lulesh_set *s, int rank, int xferFields, bool doSend, bool
 static int get_msgs(lulesh_set *s, int rank, int xferFields, bool doSend, bool planeOnly,
                     bool elems, MsgTable **out)
 {
-    CommCache &cc = g_comm[s];
+    CommCache &cc = cache_of(s);
     auto key = std::make_tuple(rank, xferFields, (int)doSend, (int)planeOnly, (int)elems);
     auto it = cc.tables.find(key);
     if (it == cc.tables.end()) {
@@ -372,7 +383,7 @@ static int node_blocks_for(lulesh_set *s, int rank, int2 **blocks, int *n)
         *n = s->n_node_blocks;
         return LULESH_OK;
     }
-    CommCache &cc = g_comm[s];
+    CommCache &cc = cache_of(s);
     auto key = std::make_tuple(rank, -1, -1, -1, -1);
     auto it = cc.tables.find(key);
     if (it == cc.tables.end()) {
@@ -408,6 +419,7 @@ static bool fields_ok(int xferFields, const int *ids, FieldList *fl)
 
 void comm_release(const lulesh_set *s)
 {
+    std::lock_guard<std::mutex> lk(g_comm_mu);
     auto it = g_comm.find(s);
     if (it == g_comm.end()) return;
     for (auto &kv : it->second.tables) {

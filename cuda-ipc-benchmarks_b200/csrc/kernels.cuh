@@ -17,9 +17,6 @@ constexpr int kNodeBlock = 128;  // threads per block, node kernels
 #ifndef LULESH_FORCE_MINB
 #define LULESH_FORCE_MINB 1
 #endif
-#ifndef LULESH_FORCECP_MINB
-#define LULESH_FORCECP_MINB 1
-#endif
 #ifndef LULESH_KIN_MINB
 #define LULESH_KIN_MINB 3
 #endif
@@ -32,7 +29,6 @@ constexpr int kNodeBlock = 128;  // threads per block, node kernels
 #define LULESH_NODAL_MINB 16
 #endif
 constexpr int kNodalMinBlocks = LULESH_NODAL_MINB;
-constexpr int kForceCpMinBlocks = LULESH_FORCECP_MINB;
 constexpr int kForceMinBlocks = LULESH_FORCE_MINB;
 constexpr int kKinMinBlocks = LULESH_KIN_MINB;
 constexpr int kEosMinBlocks = LULESH_EOS_MINB;
@@ -61,14 +57,6 @@ struct SetArgs {
 void launch_time_increment(TimeCtl *tcs, int ntc, Params P, cudaStream_t s);
 void launch_force(const SetArgs &a, int nblocks, Params P, cudaStream_t s,
                   int bs = kElemBlock);
-// corner-parallel force kernel: 8 threads per element, kCpElemsPerBlock
-// elements per block (blocks[] built with that step)
-constexpr int kCpElemsPerBlock = 32;
-void launch_force_cp(const SetArgs &a, int nblocks, Params P, cudaStream_t s);
-// 0: element per thread (k_force), 1: corner-parallel (k_force_cp)
-#ifndef LULESH_FORCE_CP
-#define LULESH_FORCE_CP 0
-#endif
 void launch_nodal(const SetArgs &a, int nblocks, Params P, cudaStream_t s,
                   int bs = kNodeBlock);
 // staged comm path: own-corner partial sums, then the update from fx/fy/fz

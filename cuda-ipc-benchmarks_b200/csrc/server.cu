@@ -91,8 +91,8 @@ struct lulesh_server {
     DomDev *ddoms = nullptr;
     int2 *dblocks = nullptr;
     size_t blocks_cap = 0;
-    int2 *cp_b = nullptr, *node_b = nullptr, *elem_b = nullptr;
-    int n_cp = 0, n_node = 0, n_elem = 0;
+    int2 *node_b = nullptr, *elem_b = nullptr;
+    int n_node = 0, n_elem = 0;
     int n_table = 0;  // domains in the launched tables
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -144,11 +144,10 @@ static int rebuild(lulesh_server *s)
                          return a->dom.numElem > b->dom.numElem;
                      });
     std::vector<DomDev> hd;
-    std::vector<int2> cb, nb, eb;
+    std::vector<int2> nb, eb;
     for (size_t d = 0; d < order.size(); ++d) {
         const DomDev &D = order[d]->dom;
         hd.push_back(D);
-        for (int i = 0; i < D.numElem; i += kCpElemsPerBlock) cb.push_back(make_int2((int)d, i));
         for (int i = 0; i < D.numNode; i += kNodeBlock) nb.push_back(make_int2((int)d, i));
         for (int i = 0; i < D.numElem; i += kElemBlock) eb.push_back(make_int2((int)d, i));
     }
@@ -164,22 +163,17 @@ static int rebuild(lulesh_server *s)
                                    cudaMemcpyHostToDevice, s->stream));
             j->fresh = false;
         }
-    const size_t need = cb.size() + nb.size() + eb.size();
+    const size_t need = nb.size() + eb.size();
     if (need > s->blocks_cap) {
         if (s->dblocks) SCHECK(cudaFreeAsync(s->dblocks, s->stream));
         size_t cap = need + need / 2 + 1024;
         SCHECK(cudaMallocAsync(&s->dblocks, sizeof(int2) * cap, s->stream));
         s->blocks_cap = cap;
     }
-    s->cp_b = s->dblocks;
-    s->node_b = s->dblocks + cb.size();
-    s->elem_b = s->dblocks + cb.size() + nb.size();
-    s->n_cp = (int)cb.size();
+    s->node_b = s->dblocks;
+    s->elem_b = s->dblocks + nb.size();
     s->n_node = (int)nb.size();
     s->n_elem = (int)eb.size();
-    if (!cb.empty())
-        SCHECK(cudaMemcpyAsync(s->cp_b, cb.data(), sizeof(int2) * cb.size(), cudaMemcpyHostToDevice,
-                               s->stream));
     if (!nb.empty())
         SCHECK(cudaMemcpyAsync(s->node_b, nb.data(), sizeof(int2) * nb.size(),
                                cudaMemcpyHostToDevice, s->stream));
@@ -197,11 +191,7 @@ static int rebuild(lulesh_server *s)
     } else {
         SCHECK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
         launch_time_increment(s->dtc, s->cfg.max_jobs, s->P, s->stream);
-#if LULESH_FORCE_CP
-        launch_force_cp(s->args(s->cp_b), s->n_cp, s->P, s->stream);
-#else
         launch_force(s->args(s->elem_b), s->n_elem, s->P, s->stream);
-#endif
         launch_nodal(s->args(s->node_b), s->n_node, s->P, s->stream);
         launch_kinematics(s->args(s->elem_b), s->n_elem, s->P, s->stream);
         launch_eos(s->args(s->elem_b), s->n_elem, s->P, s->stream);

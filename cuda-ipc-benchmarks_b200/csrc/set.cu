@@ -59,11 +59,10 @@ int build_tables(lulesh_set *s)
         std::stable_sort(dord.begin(), dord.end(), [s](int a, int b) {
             return s->hdoms[a].numElem > s->hdoms[b].numElem;
         });
-    std::vector<int2> eb, nb, gb, cb;
+    std::vector<int2> eb, nb, gb;
     for (int d : dord) {
         const DomDev &D = s->hdoms[d];
         for (int i = 0; i < D.numElem; i += s->eb) eb.push_back(make_int2(d, i));
-        for (int i = 0; i < D.numElem; i += kCpElemsPerBlock) cb.push_back(make_int2(d, i));
         for (int i = 0; i < D.numNode; i += s->nb) nb.push_back(make_int2(d, i));
         if (D.tp > 1)
             for (int f = 0; f < 6; ++f)
@@ -74,8 +73,7 @@ int build_tables(lulesh_set *s)
     s->n_elem_blocks = (int)eb.size();
     s->n_node_blocks = (int)nb.size();
     s->n_ghost_blocks = (int)gb.size();
-    s->n_cp_blocks = (int)cb.size();
-    size_t bytes = sizeof(int2) * (eb.size() + nb.size() + gb.size() + cb.size() + 1);
+    size_t bytes = sizeof(int2) * (eb.size() + nb.size() + gb.size() + 1);
     if (s->elem_blocks) {  // rebuilding: the old tables may still be in use
         LCHECK(cudaStreamSynchronize(s->stream));
         LCHECK(cudaFree(s->elem_blocks));
@@ -86,9 +84,6 @@ int build_tables(lulesh_set *s)
     s->elem_blocks = t;
     s->node_blocks = t + eb.size();
     s->ghost_blocks = t + eb.size() + nb.size();
-    s->cp_blocks = t + eb.size() + nb.size() + gb.size();
-    LCHECK(cudaMemcpyAsync(s->cp_blocks, cb.data(), sizeof(int2) * cb.size(),
-                           cudaMemcpyHostToDevice, s->stream));
     LCHECK(cudaMemcpyAsync(s->elem_blocks, eb.data(), sizeof(int2) * eb.size(),
                            cudaMemcpyHostToDevice, s->stream));
     LCHECK(cudaMemcpyAsync(s->node_blocks, nb.data(), sizeof(int2) * nb.size(),
@@ -195,11 +190,7 @@ static int create_common(lulesh_set *s, const std::vector<DomPlace> &place, int 
 
 void launch_force_fp64(lulesh_set *s, cudaStream_t st)
 {
-#if LULESH_FORCE_CP
-    launch_force_cp(s->args(s->cp_blocks), s->n_cp_blocks, s->P, st);
-#else
     launch_force(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb);
-#endif
 }
 
 int enqueue_cycle(lulesh_set *s)

@@ -38,8 +38,7 @@ struct lulesh_set {
     lulesh::TimeCtl *dtc = nullptr;
     lulesh::TimeCtl *htc_pinned = nullptr;  // pinned mirror for readback
     int2 *elem_blocks = nullptr, *node_blocks = nullptr, *ghost_blocks = nullptr;
-    int2 *cp_blocks = nullptr;  // kCpElemsPerBlock elements per block
-    int n_elem_blocks = 0, n_node_blocks = 0, n_ghost_blocks = 0, n_cp_blocks = 0;
+    int n_elem_blocks = 0, n_node_blocks = 0, n_ghost_blocks = 0;
 
     // mixed precision corner buffers
     lulesh::CornerF32 *dcorner32 = nullptr;
