@@ -3,6 +3,7 @@
 #include <climits>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -218,9 +219,57 @@ int enqueue_cycle(lulesh_set *s)
     return cuda_status(cudaGetLastError(), "cycle launch");
 }
 
+// A single domain keeps its node coordinate and velocity arrays (x..zd,
+// ~50 MB at -s 100, contiguous in the arena) persisting in L2: force reads
+// them, nodal reads and writes them, kinematics reads them again, every
+// cycle.  The access-policy window is a stream attribute, captured into
+// the cycle graph's kernel nodes.  Measured on B200 at -s 100: 339 -> 334
+// us per cycle.  Batches and subdomain sets do not use it.
+static int l2_node_window(lulesh_set *s)
+{
+    if (s->ndom != 1) return LULESH_OK;
+    const DomDev &D = s->hdoms[0];
+    const char *lo = reinterpret_cast<const char *>(D.x);
+    const char *hi = reinterpret_cast<const char *>(D.zd + D.numNode);
+    int maxwin = 0, maxpersist = 0;
+    LCHECK(cudaDeviceGetAttribute(&maxwin, cudaDevAttrMaxAccessPolicyWindowSize, s->device));
+    LCHECK(cudaDeviceGetAttribute(&maxpersist, cudaDevAttrMaxPersistingL2CacheSize, s->device));
+    if (maxwin <= 0 || maxpersist <= 0) return LULESH_OK;
+    size_t bytes = (size_t)(hi - lo);
+    if (bytes > (size_t)maxwin) bytes = (size_t)maxwin;
+    const size_t persist = bytes < (size_t)maxpersist ? bytes : (size_t)maxpersist;
+    // a limit of the process's context, released with it
+    LCHECK(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, persist));
+    cudaStreamAttrValue v{};
+    v.accessPolicyWindow.base_ptr = const_cast<char *>(lo);
+    v.accessPolicyWindow.num_bytes = bytes;
+    v.accessPolicyWindow.hitRatio = (float)((double)persist / (double)bytes);
+    v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    v.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    LCHECK(cudaStreamSetAttribute(s->stream, cudaStreamAttributeAccessPolicyWindow, &v));
+    s->l2_window = true;
+    return LULESH_OK;
+}
+
+// Remove the window from the set's stream (it may be the caller's) and
+// release the lines it made persistent.
+static void clear_l2_window(lulesh_set *s)
+{
+    if (!s->l2_window || !s->stream) return;
+    cudaStreamAttrValue v{};
+    v.accessPolicyWindow.num_bytes = 0;
+    cudaStreamSetAttribute(s->stream, cudaStreamAttributeAccessPolicyWindow, &v);
+    cudaCtxResetPersistingL2Cache();
+    s->l2_window = false;
+}
+
 static int ensure_graph(lulesh_set *s)
 {
     if (s->graph_ready) return LULESH_OK;
+    {
+        const int wst = l2_node_window(s);
+        if (wst != LULESH_OK) return wst;
+    }
     if (s->flags & LULESH_FLAG_COMM_STAGED) {
         int pst = comm_prepare(s);
         if (pst != LULESH_OK) return pst;
@@ -465,6 +514,7 @@ int lulesh_destroy(lulesh_set *s)
     if (!s) return LULESH_OK;
     if (s->stream) cudaStreamSynchronize(s->stream);
     drop_graph(s);
+    clear_l2_window(s);
     comm_release(s);
     if (s->elem_blocks) cudaFree(s->elem_blocks);
     if (s->ddoms) cudaFree(s->ddoms);
@@ -482,6 +532,7 @@ int lulesh_set_stream(lulesh_set *s, void *stream)
     if (!s) return LULESH_INVALID_ARG;
     LCHECK(cudaStreamSynchronize(s->stream));
     drop_graph(s);
+    clear_l2_window(s);
     if (s->own_stream) cudaStreamDestroy(s->stream);
     if (stream) {
         s->stream = static_cast<cudaStream_t>(stream);

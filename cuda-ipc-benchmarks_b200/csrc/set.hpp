@@ -43,6 +43,9 @@ struct lulesh_set {
     // mixed precision corner buffers
     lulesh::CornerF32 *dcorner32 = nullptr;
 
+    // L2 access-policy window set on `stream` (single domains)
+    bool l2_window = false;
+
     // the arena
     void *arena = nullptr;
     size_t arena_bytes = 0;
