@@ -140,7 +140,8 @@ int main(int argc, char *argv[])
                 st = lulesh_host_cycle(set.get(), nullptr, &s);
             }
         } else {
-            st = lulesh_run(set.get(), 256);
+            // the whole run as one graph launch (device-side loop)
+            st = lulesh_run_graph(set.get(), 0);
         }
         cudaDeviceSynchronize();
         const double elapsed = wall() - t0;

@@ -266,14 +266,8 @@ static void clear_l2_window(lulesh_set *s)
 static int ensure_graph(lulesh_set *s)
 {
     if (s->graph_ready) return LULESH_OK;
-    {
-        const int wst = l2_node_window(s);
-        if (wst != LULESH_OK) return wst;
-    }
-    if (s->flags & LULESH_FLAG_COMM_STAGED) {
-        int pst = comm_prepare(s);
-        if (pst != LULESH_OK) return pst;
-    }
+    const int pst = prepare_capture(s);
+    if (pst != LULESH_OK) return pst;
     LCHECK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
     int st = enqueue_cycle(s);
     cudaGraph_t g = nullptr;
@@ -322,6 +316,18 @@ void drop_graph(lulesh_set *s)
     s->exec = nullptr;
     s->graph = nullptr;
     s->graph_ready = false;
+    if (s->exec_run) cudaGraphExecDestroy(s->exec_run);
+    if (s->graph_run) cudaGraphDestroy(s->graph_run);
+    s->exec_run = nullptr;
+    s->graph_run = nullptr;
+}
+
+int prepare_capture(lulesh_set *s)
+{
+    const int wst = l2_node_window(s);
+    if (wst != LULESH_OK) return wst;
+    if (s->flags & LULESH_FLAG_COMM_STAGED) return comm_prepare(s);
+    return LULESH_OK;
 }
 
 static int read_states(lulesh_set *s)
@@ -349,6 +355,18 @@ static void fill_state(const TimeCtl &T, lulesh_job_state *o)
     o->deltatime = T.deltatime;
     o->dtcourant = T.dtcourant;
     o->dthydro = T.dthydro;
+}
+
+int run_status(lulesh_set *s)
+{
+    const int st = read_states(s);
+    if (st != LULESH_OK) return st;
+    for (int j = 0; j < s->njobs; ++j) {
+        lulesh_job_state o;
+        fill_state(s->htc_pinned[j], &o);
+        if (o.status != LULESH_OK) return o.status;
+    }
+    return LULESH_OK;
 }
 
 // ---- field table ----------------------------------------------------------
@@ -521,6 +539,7 @@ int lulesh_destroy(lulesh_set *s)
     if (s->dtc) cudaFree(s->dtc);
     if (s->htc_pinned) cudaFreeHost(s->htc_pinned);
     if (s->dcorner32) cudaFree(s->dcorner32);
+    if (s->run_ctl) cudaFree(s->run_ctl);
     if (s->arena) cudaFree(s->arena);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -596,12 +615,7 @@ int lulesh_run(lulesh_set *s, int check_every)
             if (!s->htc_pinned[j].done) all_done = false;
         if (all_done) break;
     }
-    for (int j = 0; j < s->njobs; ++j) {
-        lulesh_job_state o;
-        fill_state(s->htc_pinned[j], &o);
-        if (o.status != LULESH_OK) return o.status;
-    }
-    return LULESH_OK;
+    return run_status(s);
 }
 
 int lulesh_host_cycle(lulesh_set *s, const lulesh_job_state *in, lulesh_job_state *out)

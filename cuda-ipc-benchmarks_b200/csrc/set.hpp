@@ -58,6 +58,11 @@ struct lulesh_set {
     cudaGraph_t graph_k = nullptr;
     cudaGraphExec_t exec_k = nullptr;
     bool graph_k_ready = false;
+    // whole-run graph: a WHILE conditional node around one cycle
+    // (rungraph.cu); run_ctl[0] counts cycles, run_ctl[1] is the cap
+    cudaGraph_t graph_run = nullptr;
+    cudaGraphExec_t exec_run = nullptr;
+    unsigned long long *run_ctl = nullptr;
 
     // staged comm state: receive-buffer capacity per domain (doubles)
     long com_buf_doubles = 0;
@@ -92,4 +97,9 @@ int comm_prepare(lulesh_set *s);
 int build_tables(lulesh_set *s);
 // release the captured cycle graphs (rebuilt at the next step)
 void drop_graph(lulesh_set *s);
+// read every job's time state back and return the first job's non-OK
+// status (LULESH_OK when all are fine); synchronises the stream
+int run_status(lulesh_set *s);
+// prepare what enqueue_cycle needs before a capture (staged comm tables)
+int prepare_capture(lulesh_set *s);
 }  // namespace lulesh

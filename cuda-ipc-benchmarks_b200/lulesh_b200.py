@@ -65,7 +65,7 @@ EXPORTED = [
     "lulesh_server_step", "lulesh_server_poll", "lulesh_server_clock",
     "lulesh_set_graph_cycles", "lulesh_get_tuning", "lulesh_set_tuning",
     "lulesh_autotune", "lulesh_checkpoint_bytes", "lulesh_checkpoint_save",
-    "lulesh_checkpoint_load",
+    "lulesh_checkpoint_load", "lulesh_run_graph",
 ]
 
 
@@ -180,6 +180,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "lulesh_checkpoint_bytes": (ctypes.c_size_t, [vp]),
         "lulesh_checkpoint_save": (ip, [vp, vp, ctypes.c_size_t]),
         "lulesh_checkpoint_load": (ip, [vp, vp, ctypes.c_size_t]),
+        "lulesh_run_graph": (ip, [vp, ctypes.c_longlong]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -271,6 +272,14 @@ class LuleshSet:
         st = self.lib.lulesh_run(self.h, check_every)
         if st not in (OK, VOLUME_ERROR, QSTOP_ERROR):
             _check(self.lib, st, "lulesh_run")
+        return st
+
+    def run_graph(self, max_cycles: int = 0) -> int:
+        """Run to completion in one graph launch (a device-side loop over
+        cycles); status as run()."""
+        st = self.lib.lulesh_run_graph(self.h, max_cycles)
+        if st not in (OK, VOLUME_ERROR, QSTOP_ERROR):
+            _check(self.lib, st, "lulesh_run_graph")
         return st
 
     def sync(self) -> None:

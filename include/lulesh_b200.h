@@ -158,6 +158,13 @@ int lulesh_lagrange_leapfrog(lulesh_set *set);
 /* `ncycles` such cycles, asynchronously. */
 int lulesh_step(lulesh_set *set, int ncycles);
 
+/* The whole run in one CUDA graph launch: a WHILE conditional node repeats
+ * the cycle until every job of the set is done (the reference's host loop,
+ * lulesh.cu:4858-4873, moved onto the device).  max_cycles bounds the loop
+ * (<= 0: 1,000,000 cycles); jobs still running when it stops are left as
+ * they are.  Synchronous; returns like lulesh_run. */
+int lulesh_run_graph(lulesh_set *set, long long max_cycles);
+
 /* Capture k consecutive cycles in one CUDA graph (default 1): lulesh_step(n)
  * then issues n / k launches of the k-cycle graph and n % k of the
  * one-cycle graph, so a whole batch run can be a single graph launch. */
