@@ -312,6 +312,9 @@ def run_ours(a, rank, world, local_rank):
         import batching
 
         batch_res = batching.run_batch_vs_plain(batching.config3_jobs(n=a.batch_jobs))
+    unstructured_res = None
+    if world == 1 and a.unstructured > 0:
+        unstructured_res = unstructured_vs_structured(a.unstructured, 200, 5)
     cpu = cpu_baseline_sample() if world == 1 else None
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
@@ -344,7 +347,48 @@ def run_ours(a, rank, world, local_rank):
         "cpu_baseline": cpu,
         "serving": serving_res, "batch": batch_res,
     }
+    if unstructured_res is not None:
+        line["unstructured"] = unstructured_res
     print(json.dumps(line), flush=True)
+
+
+def unstructured_vs_structured(nx, steps, warmup):
+    """The -s nx cube written as an lmesh file and run through the
+    unstructured kernels (mesh tables read from HBM) against the -s nx run
+    (tables computed from the element index): device time per cycle."""
+    import tempfile
+
+    import torch
+    import lmesh
+    import lulesh_b200 as L
+
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    out = {"nx": nx, "zones": nx ** 3, "steps": steps, "warmup": warmup}
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, f"box{nx}.lmesh")
+        lmesh.write(path, lmesh.box(nx))
+        for kind in ("structured", "unstructured"):
+            s = (L.LuleshSet(nx=nx, its=-1) if kind == "structured"
+                 else L.LuleshSet.from_mesh(path, its=-1))
+            s.set_stream(stream.cuda_stream)
+            s.step(warmup)
+            torch.cuda.synchronize()
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            s.step(steps)
+            t1.record(stream)
+            torch.cuda.synchronize()
+            ms = t0.elapsed_time(t1)
+            out[kind] = {"ms_per_cycle": ms / steps,
+                         "zone_cycles_per_s": nx ** 3 * steps / (ms / 1e3),
+                         "phases_ms": s.profile_phases(5)}
+            s.close()
+    # (energies agree only at nx = 45, where the -s deposit equals the
+    # lmesh one; the bit-for-bit comparison is a GPU test)
+    out["ratio"] = out["unstructured"]["zone_cycles_per_s"] / out["structured"]["zone_cycles_per_s"]
+    return out
 
 
 def run_reference(a, rank, world):
@@ -391,6 +435,8 @@ def main():
                     help="jobs of the serving stream (2000 = the full stream; 0 skips)")
     ap.add_argument("--batch-jobs", dest="batch_jobs", type=int, default=64,
                     help="jobs of the batch comparison (0 skips)")
+    ap.add_argument("--unstructured", type=int, default=0,
+                    help="also time the -s N cube read as an lmesh file (0 skips)")
     a = ap.parse_args()
     if a.warmup < 3:
         ap.error("--warmup must be >= 3")

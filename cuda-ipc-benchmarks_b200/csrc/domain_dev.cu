@@ -22,6 +22,22 @@ DomSizes sizes_of(int nx, int numReg, long comm_doubles)
     return s;
 }
 
+DomSizes sizes_of(const HostDomain &h, long comm_doubles)
+{
+    if (!h.unstructured) return sizes_of(h.nx, h.numReg, comm_doubles);
+    DomSizes s;
+    s.E = (size_t)h.numElem;
+    s.N = (size_t)h.numNode;
+    s.Ep = (size_t)h.Ep;
+    s.allElem = s.E;
+    s.corner = 8 * s.E;
+    s.en2 = h.symmX.size();
+    s.nr = (size_t)h.numReg;
+    s.comm = 0;
+    s.unstructured = true;
+    return s;
+}
+
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 size_t domain_bytes(const DomSizes &s, bool mixed)
@@ -39,6 +55,7 @@ size_t domain_bytes(const DomSizes &s, bool mixed)
     b += 3 * align256(4 * s.nr);        // regCSR, regReps, regSorted
     if (s.comm) b += align256(8 * s.comm);
     if (mixed) b += 3 * align256(4 * 8 * s.Ep);
+    if (s.unstructured) b += align256(4 * s.N);  // nodeBC
     return b;
 }
 
@@ -71,7 +88,7 @@ static int upload(T *dst, const std::vector<T> &src, cudaStream_t s)
 int upload_domain(const HostDomain &h, int tc, long comm_doubles, bool mixed, Carver &cv,
                   cudaStream_t st, DomDev *out, CornerF32 *c32)
 {
-    const DomSizes z = sizes_of(h.nx, h.numReg, comm_doubles);
+    const DomSizes z = sizes_of(h, comm_doubles);
     DomDev D{};
     D.nx = h.nx;
     D.en = h.nx + 1;
@@ -128,6 +145,9 @@ int upload_domain(const HostDomain &h, int tc, long comm_doubles, bool mixed, Ca
         D.commRecv = cv.take<double>(z.comm);
         D.commRecvLen = (long)z.comm;
     }
+    D.unstructured = h.unstructured ? 1 : 0;
+    D.octant = h.octantCorner;
+    if (h.unstructured) D.nodeBC = cv.take<int>(z.N);
     if (mixed && c32) {
         c32->fx = cv.take<float>(8 * z.Ep);
         c32->fy = cv.take<float>(8 * z.Ep);
@@ -184,6 +204,7 @@ int upload_domain(const HostDomain &h, int tc, long comm_doubles, bool mixed, Ca
                  D.regCSR, D.regReps, D.regSorted, D.eosOrder};
     for (size_t k = 0; k < sizeof(ip) / sizeof(ip[0]); ++k)
         if ((su = upload(ip[k], *iv[k], st)) != LULESH_OK) return su;
+    if (h.unstructured && (su = upload(D.nodeBC, h.nodeBC, st)) != LULESH_OK) return su;
     // the host vectors must outlive the asynchronous copies
     DCHECK(cudaStreamSynchronize(st));
     *out = D;

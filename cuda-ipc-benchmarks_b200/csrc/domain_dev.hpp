@@ -13,9 +13,12 @@ namespace lulesh {
 
 struct DomSizes {
     size_t E, N, Ep, allElem, corner, en2, nr, comm;
+    bool unstructured = false;  // adds the per-node boundary mask
 };
 
 DomSizes sizes_of(int nx, int numReg, long comm_doubles);
+// sizes of a host-built domain (structured or read from an lmesh file)
+DomSizes sizes_of(const HostDomain &h, long comm_doubles);
 size_t align256(size_t b);
 // device bytes of one domain (all of its arrays at 256-byte alignment)
 size_t domain_bytes(const DomSizes &s, bool mixed);

@@ -56,8 +56,14 @@ struct VelRegs {
 // The eight node indices of element el on the structured mesh, in the
 // nodelist order of BuildMesh (lulesh.cu:730-737): corner j sits at lattice
 // offset (x: bits 0x66, y: 0xCC, z: 0xF0 of j) from corner 0.
+template <bool U = false>
 __device__ __forceinline__ void elem_nodes(const DomDev &D, int el, int n[8])
 {
+    if (U) {  // an unstructured mesh's own nodelist (stride padded_numElem)
+#pragma unroll
+        for (int k = 0; k < 8; ++k) n[k] = D.nodelist[(size_t)k * D.Ep + el];
+        return;
+    }
     const int nx = D.nx, en = D.en;
     const int ix = el % nx;
     const int t = el / nx;

@@ -4,6 +4,8 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <cstdio>
+#include <string>
 
 namespace lulesh {
 
@@ -113,6 +115,27 @@ Params default_params()
 static inline double lattice(int g, int edge)
 {
     return 1.125 * (double)g / (double)edge;
+}
+
+// node -> corner CSR from the nodelist, outer corner j, inner element
+// (lulesh.cu:1054-1106)
+static void build_corner_csr(HostDomain &d)
+{
+    const int E = d.numElem, N = d.numNode, Ep = d.Ep;
+    d.nodeElemCount.assign(N, 0);
+    d.nodeElemStart.assign(N, 0);
+    for (int i = 0; i < E; ++i)
+        for (int j = 0; j < 8; ++j) d.nodeElemCount[d.nodelist[(size_t)j * Ep + i]]++;
+    for (int i = 1; i < N; ++i)
+        d.nodeElemStart[i] = d.nodeElemStart[i - 1] + d.nodeElemCount[i - 1];
+    d.nodeElemCornerList.assign((size_t)d.nodeElemStart[N - 1] + d.nodeElemCount[N - 1], 0);
+    std::vector<int> fill(N, 0);
+    for (int j = 0; j < 8; ++j)
+        for (int i = 0; i < E; ++i) {
+            int m = d.nodelist[(size_t)j * Ep + i];
+            d.nodeElemCornerList[d.nodeElemStart[m] + fill[m]] = Ep * j + i;
+            fill[m]++;
+        }
 }
 
 // ---- regions: CreateRegionIndexSets + sortRegions, lulesh.cu:1224-1398 ----
@@ -385,21 +408,7 @@ void build_domain(HostDomain &d, int nx, int tp, int col, int row, int plane,
         }
     }
 
-    // node -> corner CSR, outer corner j, inner element (lulesh.cu:1054-1106)
-    d.nodeElemCount.assign(N, 0);
-    d.nodeElemStart.assign(N, 0);
-    for (int i = 0; i < E; ++i)
-        for (int j = 0; j < 8; ++j) d.nodeElemCount[d.nodelist[(size_t)j * Ep + i]]++;
-    for (int i = 1; i < N; ++i)
-        d.nodeElemStart[i] = d.nodeElemStart[i - 1] + d.nodeElemCount[i - 1];
-    d.nodeElemCornerList.assign((size_t)d.nodeElemStart[N - 1] + d.nodeElemCount[N - 1], 0);
-    std::vector<int> fill(N, 0);
-    for (int j = 0; j < 8; ++j)
-        for (int i = 0; i < E; ++i) {
-            int m = d.nodelist[(size_t)j * Ep + i];
-            d.nodeElemCornerList[d.nodeElemStart[m] + fill[m]] = Ep * j + i;
-            fill[m]++;
-        }
+    build_corner_csr(d);
     d.matElemlist.resize(E);
     for (int i = 0; i < E; ++i) d.matElemlist[i] = i;
 
@@ -465,6 +474,169 @@ void build_domain(HostDomain &d, int nx, int tp, int col, int row, int plane,
     d.deltatime = (.5 * cbrt(d.volo[0])) / sqrt(2 * d.einit);
 
     build_regions(d, numReg, balance);
+}
+
+// ---- unstructured input (lmesh) --------------------------------------------
+
+namespace {
+
+// whitespace-separated integers and doubles of an lmesh file
+struct LmeshReader {
+    std::FILE *f = nullptr;
+    bool ok = true;
+    ~LmeshReader()
+    {
+        if (f) std::fclose(f);
+    }
+    int i()
+    {
+        int v = 0;
+        if (ok && std::fscanf(f, "%d", &v) != 1) ok = false;
+        return v;
+    }
+    double r()
+    {
+        double v = 0;
+        if (ok && std::fscanf(f, "%lf", &v) != 1) ok = false;
+        return v;
+    }
+};
+
+// boundary bits of every element whose whole face lies in the node set
+// (the face tests of lulesh.cu:1001-1012); m/p = bits of the min/max faces
+void mark_faces(const HostDomain &d, const std::vector<char> &in_set, int zm, int zp, int em,
+                int ep, int xm, int xp, std::vector<int> &bc)
+{
+    for (int z = 0; z < d.numElem; ++z) {
+        int mask = 0;
+        for (int k = 0; k < 8; ++k)
+            mask |= (in_set[d.nodelist[(size_t)k * d.Ep + z]] ? 1 : 0) << k;
+        if ((mask & 0x0f) == 0x0f) bc[z] |= zm;
+        if ((mask & 0xf0) == 0xf0) bc[z] |= zp;
+        if ((mask & 0x33) == 0x33) bc[z] |= em;
+        if ((mask & 0xcc) == 0xcc) bc[z] |= ep;
+        if ((mask & 0x99) == 0x99) bc[z] |= xm;
+        if ((mask & 0x66) == 0x66) bc[z] |= xp;
+    }
+}
+
+}  // namespace
+
+bool build_domain_lmesh(HostDomain &d, const char *path, int numReg, int balance, int cost,
+                        std::string *err)
+{
+    auto fail = [&](const std::string &m) {
+        if (err) *err = std::string("lmesh ") + path + ": " + m;
+        return false;
+    };
+    LmeshReader in;
+    in.f = std::fopen(path, "r");
+    if (!in.f) return fail("cannot open");
+    const int E = in.i(), N = in.i();
+    if (!in.ok || E < 1 || N < 8 || E > (1 << 27) || N > (1 << 28))
+        return fail("bad element/node counts");
+    d = HostDomain{};
+    d.unstructured = true;
+    d.nx = 0;
+    d.en = 0;
+    d.tp = 1;
+    d.cost = cost;
+    d.numElem = E;
+    d.numNode = N;
+    d.Ep = ((E + 31) / 32) * 32;
+    d.allElem = E;
+    for (int f = 0; f < 6; ++f) d.ghost[f] = -1;
+    d.x.resize(N);
+    d.y.resize(N);
+    d.z.resize(N);
+    for (int n = 0; n < N; ++n) {
+        d.x[n] = in.r();
+        d.y[n] = in.r();
+        d.z[n] = in.r();
+    }
+    d.nodelist.assign(8 * (size_t)d.Ep, 0);
+    for (int z = 0; z < E; ++z)
+        for (int k = 0; k < 8; ++k) {
+            const int n = in.i();
+            if (n < 0 || n >= N) return fail("node id out of range in element " + std::to_string(z));
+            d.nodelist[(size_t)k * d.Ep + z] = n;
+        }
+    std::vector<int> *links[6] = {&d.lxim, &d.lxip, &d.letam, &d.letap, &d.lzetam, &d.lzetap};
+    for (auto *l : links) l->resize(E);
+    for (int z = 0; z < E; ++z)
+        for (auto *l : links) {
+            const int v = in.i();
+            if (v < 0 || v >= E) return fail("face neighbour out of range in element " +
+                                             std::to_string(z));
+            (*l)[z] = v;
+        }
+    std::vector<int> *sets[3] = {&d.symmX, &d.symmY, &d.symmZ};
+    int *counts[3] = {&d.numSymmX, &d.numSymmY, &d.numSymmZ};
+    d.nodeBC.assign(N, 0);
+    std::vector<char> symm(N, 0), freesurf(N, 0);
+    for (int a = 0; a < 3; ++a) {
+        const int c = in.i();
+        if (!in.ok || c < 0 || c > N) return fail("bad symmetry set size");
+        *counts[a] = c;
+        sets[a]->resize(c);
+        for (int k = 0; k < c; ++k) {
+            const int n = in.i();
+            if (n < 0 || n >= N) return fail("symmetry node out of range");
+            (*sets[a])[k] = n;
+            symm[n] = 1;
+            d.nodeBC[n] |= 1 << a;
+        }
+    }
+    const int nfree = in.i();
+    if (!in.ok || nfree < 0 || nfree > N) return fail("bad free-surface set size");
+    for (int k = 0; k < nfree; ++k) {
+        const int n = in.i();
+        if (n < 0 || n >= N) return fail("free-surface node out of range");
+        freesurf[n] = 1;
+    }
+    if (!in.ok) return fail("truncated");
+    // device arrays of the symmetry sets share one size
+    int en2 = 1;
+    for (int a = 0; a < 3; ++a) en2 = std::max(en2, *counts[a]);
+    for (auto *v : sets) v->resize(en2, 0);
+
+    d.elemBC.assign(E, 0);
+    mark_faces(d, symm, ZETA_M_SYMM, ZETA_P_SYMM, ETA_M_SYMM, ETA_P_SYMM, XI_M_SYMM, XI_P_SYMM,
+               d.elemBC);
+    d.octantCorner = 0;
+    for (int z = 0; z < E; ++z)
+        if (d.elemBC[z] == (XI_M_SYMM | ETA_M_SYMM | ZETA_M_SYMM)) {
+            d.octantCorner = z;
+            break;
+        }
+    mark_faces(d, freesurf, ZETA_M_FREE, ZETA_P_FREE, ETA_M_FREE, ETA_P_FREE, XI_M_FREE,
+               XI_P_FREE, d.elemBC);
+
+    build_corner_csr(d);
+    d.matElemlist.resize(E);
+    for (int z = 0; z < E; ++z) d.matElemlist[z] = z;
+    d.volo.resize(E);
+    d.elemMass.resize(E);
+    d.nodalMass.assign(N, 0.0);
+    for (int z = 0; z < E; ++z) {
+        double xl[8], yl[8], zl[8];
+        for (int k = 0; k < 8; ++k) {
+            const int g = d.nodelist[(size_t)k * d.Ep + z];
+            xl[k] = d.x[g];
+            yl[k] = d.y[g];
+            zl[k] = d.z[g];
+        }
+        const double vol = elem_volume_host(xl, yl, zl);
+        d.volo[z] = vol;
+        d.elemMass[z] = vol;
+        for (int k = 0; k < 8; ++k) d.nodalMass[d.nodelist[(size_t)k * d.Ep + z]] += vol / 8.0;
+    }
+    d.e.assign(E, 0.0);
+    d.einit = 3.948746e+7;
+    d.e[d.octantCorner] = d.einit;
+    d.deltatime = (.5 * cbrt(d.volo[d.octantCorner])) / sqrt(2 * d.einit);
+    build_regions(d, numReg, balance);
+    return true;
 }
 
 void build_domain_light(HostDomain &d, int nx, int numReg, int balance, int cost)

@@ -7,6 +7,7 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
 #include <vector>
 
 #include "lulesh_dev.h"
@@ -50,6 +51,10 @@ struct HostDomain {
     // geometry and connectivity left to the device (build_domain_light):
     // the vectors from nodelist to nodalMass above are empty
     bool device_geometry = false;
+    // read from an lmesh file (build_domain_lmesh)
+    bool unstructured = false;
+    int octantCorner = 0;
+    std::vector<int> nodeBC;  // per node: bit 0/1/2 = in symmX/Y/Z
 };
 
 // Reference parameter block, lulesh.cu:1125-1158.
@@ -69,6 +74,20 @@ void build_domain(HostDomain &d, int nx, int tp, int col, int row, int plane,
 // generated on the device (setup.cu) with the same values build_domain
 // computes.
 void build_domain_light(HostDomain &d, int nx, int numReg, int balance, int cost);
+
+// An unstructured domain from an lmesh file, the format the reference reads
+// with -u (lulesh.cu:855-1052): "numElem numNode", the node coordinates, 8
+// node ids per element, 6 face neighbours per element (xi-, xi+, eta-,
+// eta+, zeta-, zeta+), then the X, Y, Z symmetry node sets and the free
+// surface node set, each as a count followed by the ids.  Boundary masks
+// follow the reference's face tests on those sets, with one correction:
+// faces on the free surface get the *_FREE bits (the reference's reader
+// marks them *_SYMM, lulesh.cu:1039-1044).  The energy 3.948746e7 goes to
+// the octant corner (the first element with all three minimum faces on
+// symmetry planes, lulesh.cu:1015-1022) and the initial dt follows from
+// that element's volume.  Returns false with *err set on a malformed file.
+bool build_domain_lmesh(HostDomain &d, const char *path, int numReg, int balance, int cost,
+                        std::string *err);
 
 // CalcElemVolume (lulesh.cu:221-307), host copy used at setup.
 double elem_volume_host(const double *x, const double *y, const double *z);

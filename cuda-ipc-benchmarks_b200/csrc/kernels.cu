@@ -112,7 +112,7 @@ __device__ __constant__ int kCZ[8] = {0, 0, 0, 0, 1, 1, 1, 1};
 // ---------------------------------------------------------------------------
 // force: CalcVolumeForceForElems_kernel, lulesh.cu:2080-2259
 
-template <bool HG, int BS>
+template <bool HG, int BS, bool U>
 __global__ void __launch_bounds__(BS, min_blocks(kForceMinBlocks, BS)) k_force(SetArgs a, Params P)
 {
     const int2 blk = a.blocks[blockIdx.x];
@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(BS, min_blocks(kForceMinBlocks, BS)) k_force(S
     // loads then overlap the coordinate work instead of stalling the
     // hourglass step (measured on B200 at -s 100: 150 -> 136 us)
     int n[8];
-    elem_nodes(D, elem, n);
+    elem_nodes<U>(D, elem, n);
     double xn[8], yn[8], zn[8];
     double xdn[8], ydn[8], zdn[8];
 #pragma unroll
@@ -149,17 +149,21 @@ __global__ void __launch_bounds__(BS, min_blocks(kForceMinBlocks, BS)) k_force(S
     force_elem<HG>(D, T, P, elem, xn, yn, zn, vel);
 }
 
-template <int BS>
+template <int BS, bool U = false>
 static void launch_force_bs(const SetArgs &a, int nblocks, Params P, cudaStream_t s)
 {
     if (P.hgcoef > 0.0)
-        k_force<true, BS><<<nblocks, BS, 0, s>>>(a, P);
+        k_force<true, BS, U><<<nblocks, BS, 0, s>>>(a, P);
     else
-        k_force<false, BS><<<nblocks, BS, 0, s>>>(a, P);
+        k_force<false, BS, U><<<nblocks, BS, 0, s>>>(a, P);
 }
 
-void launch_force(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs)
+void launch_force(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs, bool u)
 {
+    if (u) {
+        launch_force_bs<kElemBlock, true>(a, nblocks, P, s);
+        return;
+    }
     switch (bs) {
         case 64: launch_force_bs<64>(a, nblocks, P, s); break;
         case 256: launch_force_bs<256>(a, nblocks, P, s); break;
@@ -213,7 +217,7 @@ __device__ __forceinline__ void gather_corners(const DomDev *doms, const DomDev 
 // MODE 1: AddNodeForcesFromElems over this domain's own corners only,
 //         writing fx/fy/fz (the partial sums the reference exchanges).
 // MODE 2: the node update from fx/fy/fz (after CommSBN added neighbours).
-template <int MODE, int BS>
+template <int MODE, int BS, bool U = false>
 __global__ void __launch_bounds__(BS, min_blocks(kNodalMinBlocks, BS)) k_nodal(SetArgs a, Params P)
 {
     const int2 blk = a.blocks[blockIdx.x];
@@ -222,14 +226,28 @@ __global__ void __launch_bounds__(BS, min_blocks(kNodalMinBlocks, BS)) k_nodal(S
     if (!T.active) return;
     const int i = blk.y + threadIdx.x;
     if (i >= D.numNode) return;
-    const int en = D.en;
-    const int px = i % en;
-    const int t = i / en;
-    const int py = t % en;
-    const int pz = t / en;
+    int px = 0, py = 0, pz = 0;
+    if (!U) {
+        const int en = D.en;
+        px = i % en;
+        const int t = i / en;
+        py = t % en;
+        pz = t / en;
+    }
 
     double fx, fy, fz;
-    if (MODE == 0) {
+    if (MODE == 0 && U) {
+        // AddNodeForcesFromElems (lulesh.cu:1715-1751): the node's corners
+        // in nodeElemCornerList order
+        fx = fy = fz = 0.0;
+        const int start = D.nodeElemStart[i], count = D.nodeElemCount[i];
+        for (int j = 0; j < count; ++j) {
+            const int k = D.nodeElemCornerList[start + j];
+            fx += ld_corner(D.fx_elem + k);
+            fy += ld_corner(D.fy_elem + k);
+            fz += ld_corner(D.fz_elem + k);
+        }
+    } else if (MODE == 0) {
         gather_corners(a.doms, D, px, py, pz, fx, fy, fz);
     } else if (MODE == 1) {
         DomDev L = D;
@@ -251,10 +269,18 @@ __global__ void __launch_bounds__(BS, min_blocks(kNodalMinBlocks, BS)) k_nodal(S
     double ydd = fy * one_over_nMass;
     double zdd = fz * one_over_nMass;
     // ApplyAccelerationBoundaryConditionsForNodes: symmetry planes are the
-    // px/py/pz == 0 node sets of the domains at the mesh origin faces
-    if (D.col == 0 && px == 0) xdd = 0.0;
-    if (D.row == 0 && py == 0) ydd = 0.0;
-    if (D.plane == 0 && pz == 0) zdd = 0.0;
+    // px/py/pz == 0 node sets of the domains at the mesh origin faces (an
+    // unstructured mesh lists its symmetry nodes: nodeBC bits)
+    if (U) {
+        const int m = D.nodeBC[i];
+        if (m & 1) xdd = 0.0;
+        if (m & 2) ydd = 0.0;
+        if (m & 4) zdd = 0.0;
+    } else {
+        if (D.col == 0 && px == 0) xdd = 0.0;
+        if (D.row == 0 && py == 0) ydd = 0.0;
+        if (D.plane == 0 && pz == 0) zdd = 0.0;
+    }
 
     // CalcPositionAndVelocityForNodes_kernel, lulesh.cu:2999-3028
     const double dt = T.deltatime;
@@ -283,8 +309,12 @@ __global__ void __launch_bounds__(BS, min_blocks(kNodalMinBlocks, BS)) k_nodal(S
     }
 }
 
-void launch_nodal(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs)
+void launch_nodal(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs, bool u)
 {
+    if (u) {
+        k_nodal<0, kNodeBlock, true><<<nblocks, kNodeBlock, 0, s>>>(a, P);
+        return;
+    }
     switch (bs) {
         case 256: k_nodal<0, 256><<<nblocks, 256, 0, s>>>(a, P); break;
         case 512: k_nodal<0, 512><<<nblocks, 512, 0, s>>>(a, P); break;
@@ -305,7 +335,7 @@ void launch_nodal_update(const SetArgs &a, int nblocks, Params P, cudaStream_t s
 // ---------------------------------------------------------------------------
 // kinematics: CalcKinematicsAndMonotonicQGradient_kernel, lulesh.cu:3343-3507
 
-template <int BS>
+template <int BS, bool U = false>
 __global__ void __launch_bounds__(BS, min_blocks(kKinMinBlocks, BS)) k_kinematics(SetArgs a)
 {
     const int2 blk = a.blocks[blockIdx.x];
@@ -317,7 +347,7 @@ __global__ void __launch_bounds__(BS, min_blocks(kKinMinBlocks, BS)) k_kinematic
 
     // all node gathers first (measured on B200 at -s 100: 92 -> 84 us)
     int nodes[8];
-    elem_nodes(D, k, nodes);
+    elem_nodes<U>(D, k, nodes);
     double x_local[8], y_local[8], z_local[8];
     double xd_local[8], yd_local[8], zd_local[8];
 #pragma unroll
@@ -336,9 +366,13 @@ __global__ void __launch_bounds__(BS, min_blocks(kKinMinBlocks, BS)) k_kinematic
     kin_elem(D, T, k, x_local, y_local, z_local, vel);
 }
 
-void launch_kinematics(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs)
+void launch_kinematics(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs, bool u)
 {
     (void)P;
+    if (u) {
+        k_kinematics<kElemBlock, true><<<nblocks, kElemBlock, 0, s>>>(a);
+        return;
+    }
     switch (bs) {
         case 64: k_kinematics<64><<<nblocks, 64, 0, s>>>(a); break;
         case 256: k_kinematics<256><<<nblocks, 256, 0, s>>>(a); break;
@@ -511,7 +545,7 @@ __device__ __forceinline__ double warp_min(double v)
     return v;
 }
 
-template <int BS>
+template <int BS, bool U = false>
 __global__ void __launch_bounds__(BS, min_blocks(kEosMinBlocks, BS)) k_eos(SetArgs a, Params P)
 {
     const int2 blk = a.blocks[blockIdx.x];
@@ -535,7 +569,17 @@ __global__ void __launch_bounds__(BS, min_blocks(kEosMinBlocks, BS)) k_eos(SetAr
         // ---- CalcMonotonicQRegionForElems_kernel, lulesh.cu:3586-3724
         const double ptiny = 1.e-36;
         int bcMask, lxm, lxp, lem, lep, lzm, lzp;
-        elem_face_links(D, zidx, bcMask, lxm, lxp, lem, lep, lzm, lzp);
+        if (U) {  // the mesh's own links and boundary mask
+            bcMask = D.elemBC[zidx];
+            lxm = D.lxim[zidx];
+            lxp = D.lxip[zidx];
+            lem = D.letam[zidx];
+            lep = D.letap[zidx];
+            lzm = D.lzetam[zidx];
+            lzp = D.lzetap[zidx];
+        } else {
+            elem_face_links(D, zidx, bcMask, lxm, lxp, lem, lep, lzm, lzp);
+        }
         const double mult = P.monoq_limiter_mult, maxs = P.monoq_max_slope;
         const double phixi =
             mono_limiter(D.delv_xi, zidx, bcMask, XI_M, XI_M_SYMM, XI_M_FREE, XI_P, XI_P_SYMM,
@@ -683,8 +727,12 @@ __global__ void __launch_bounds__(BS, min_blocks(kEosMinBlocks, BS)) k_eos(SetAr
     }
 }
 
-void launch_eos(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs)
+void launch_eos(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs, bool u)
 {
+    if (u) {
+        k_eos<kElemBlock, true><<<nblocks, kElemBlock, 0, s>>>(a, P);
+        return;
+    }
     switch (bs) {
         case 64: k_eos<64><<<nblocks, 64, 0, s>>>(a, P); break;
         case 256: k_eos<256><<<nblocks, 256, 0, s>>>(a, P); break;

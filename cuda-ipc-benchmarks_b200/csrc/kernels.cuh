@@ -28,8 +28,7 @@ constexpr int kNodeBlock = 128;  // threads per block, node kernels
 #ifndef LULESH_NODAL_MINB
 #define LULESH_NODAL_MINB 16
 #endif
-constexpr int kNodalMinBlocks = LULESH_NODAL_MINB;
-constexpr int kForceMinBlocks = LULESH_FORCE_MINB;
+constexpr int kNodalMinBlocks = LULESH_NODAL_MINB;constexpr int kForceMinBlocks = LULESH_FORCE_MINB;
 constexpr int kKinMinBlocks = LULESH_KIN_MINB;
 constexpr int kEosMinBlocks = LULESH_EOS_MINB;
 
@@ -55,16 +54,19 @@ struct SetArgs {
 };
 
 void launch_time_increment(TimeCtl *tcs, int ntc, Params P, cudaStream_t s);
+// u: the set's domains are unstructured (lmesh): 128-wide blocks, mesh
+// arrays read instead of structured indexing
 void launch_force(const SetArgs &a, int nblocks, Params P, cudaStream_t s,
-                  int bs = kElemBlock);
+                  int bs = kElemBlock, bool u = false);
 void launch_nodal(const SetArgs &a, int nblocks, Params P, cudaStream_t s,
-                  int bs = kNodeBlock);
+                  int bs = kNodeBlock, bool u = false);
 // staged comm path: own-corner partial sums, then the update from fx/fy/fz
 void launch_nodal_gather_local(const SetArgs &a, int nblocks, cudaStream_t s);
 void launch_nodal_update(const SetArgs &a, int nblocks, Params P, cudaStream_t s);
 void launch_kinematics(const SetArgs &a, int nblocks, Params P, cudaStream_t s,
-                       int bs = kElemBlock);
-void launch_eos(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs = kElemBlock);
+                       int bs = kElemBlock, bool u = false);
+void launch_eos(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs = kElemBlock,
+                bool u = false);
 // fused halo kernels of a subdomain set (direct reads of neighbour memory)
 void launch_posvel_sync(const SetArgs &a, int nblocks, cudaStream_t s);
 void launch_monoq_ghost(const SetArgs &a, int nblocks, cudaStream_t s);

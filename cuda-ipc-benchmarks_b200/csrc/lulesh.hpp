@@ -58,6 +58,13 @@ class DomainSet {
         check(lulesh_create(&j, tp, flags, device, &set_), "NewDomain");
         tp_ = tp;
     }
+    // NewDomain's unstructured branch: one domain read from an lmesh file
+    DomainSet(const char *mesh, int nr, int balance, int cost, int its, int flags,
+              int device = -1)
+    {
+        lulesh_job j{1, nr, balance, cost, its};
+        check(lulesh_create_from_mesh(mesh, &j, flags, device, &set_), "NewDomain");
+    }
     ~DomainSet() { release(); }
     // free every device resource now (the destructor then does nothing)
     void release()

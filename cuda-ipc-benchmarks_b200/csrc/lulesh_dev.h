@@ -83,6 +83,12 @@ struct DomDev {
     // comm message buffers (staged exchange): receive buffer of this rank
     double *commRecv;
     long commRecvLen;
+    // unstructured (lmesh) domains: kernels read nodelist, the corner CSR,
+    // the face links and elemBC instead of computing them from the element
+    // position; nodeBC[n] has bit 0/1/2 set when node n is in symmX/Y/Z
+    int unstructured;
+    int octant;  // element holding the energy deposit (0 on -s meshes)
+    int *nodeBC;
 };
 
 // Mixed-precision corner forces, FP32, layout of fx_elem ([8][Ep]).

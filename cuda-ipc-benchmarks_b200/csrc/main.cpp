@@ -2,6 +2,7 @@
 //
 // Accepts both forms of the reference command line:
 //   CUDA form  lulesh -s N [x ITERS]       (LULESH/cuda/src/lulesh.cu:4754-4770;
+//              -u FILE.lmesh in place of -s N reads an unstructured mesh;
 //              a 4th positional argument is the iteration count, so both
 //              "-s 45 -i 100" and the harness form "-s 45 0 200" work)
 //   omp form   -s -i -r -b -c -p -q -f -v -z -h (LULESH/omp_4.0/lulesh-util.cc:60-173)
@@ -39,7 +40,7 @@ static void usage(const char *exe)
     std::printf(" --mixed         : FP32 element arithmetic, FP64 EOS/integration/dt\n");
     std::printf(" --no-xyz        : do not write xyz.asc\n");
     std::printf(" -h              : This message\n");
-    std::printf("Unstructured meshes (-u) are not supported by this build.\n");
+    std::printf(" -u <file.lmesh> : read an unstructured mesh instead of -s\n");
 }
 
 static bool to_int(const char *s, int *v)
@@ -64,15 +65,15 @@ int main(int argc, char *argv[])
     const double t_app_start = wall();
     int nx = 30, its = -1, nr = 11, balance = 1, cost = 1, tp = 1;
     bool quiet = false, progress = false, staged = false, mixed = false, xyz = true;
-    if (argc >= 2 && std::strcmp(argv[1], "-u") == 0) {
-        std::printf("Unstructured mesh input (-u) is not supported by this build\n");
-        return LFileError;
-    }
-    // CUDA form: exactly "-s N x ITERS" (argc == 5, argv[4] the count)
-    bool cuda_form = (argc == 5 && std::strcmp(argv[1], "-s") == 0 &&
+    std::string mesh;  // -u: an lmesh file
+    // CUDA form: exactly "-s N x ITERS" or "-u FILE x ITERS" (argc == 5,
+    // argv[4] the count)
+    const bool u_form = argc >= 2 && std::strcmp(argv[1], "-u") == 0;
+    bool cuda_form = (argc == 5 && (std::strcmp(argv[1], "-s") == 0 || u_form) &&
                       std::strcmp(argv[3], "-i") != 0 && argv[3][0] != '-');
     if (cuda_form) {
-        if (!to_int(argv[2], &nx) || !to_int(argv[4], &its)) {
+        if (u_form) mesh = argv[2];
+        if ((!u_form && !to_int(argv[2], &nx)) || !to_int(argv[4], &its)) {
             usage(argv[0]);
             return LFileError;
         }
@@ -88,6 +89,13 @@ int main(int argc, char *argv[])
                 ++i;
             };
             if (a == "-s") need(&nx);
+            else if (a == "-u") {
+                if (i + 1 >= argc) {
+                    usage(argv[0]);
+                    return LFileError;
+                }
+                mesh = argv[++i];
+            }
             else if (a == "-i") need(&its);
             else if (a == "-r") need(&nr);
             else if (a == "-b") need(&balance);
@@ -114,13 +122,26 @@ int main(int argc, char *argv[])
     }
     if (its == 0) its = -1;  // "-s N 0 ITERS": 0 means no cap in that slot
     int flags = (staged ? LULESH_FLAG_COMM_STAGED : 0) | (mixed ? LULESH_FLAG_MIXED : 0);
+    const bool structured = mesh.empty();
+    if (!structured && tp != 1) {
+        std::printf("an unstructured mesh runs as one domain (-t 1)\n");
+        return LFileError;
+    }
     try {
-        DomainSet set(nx, tp, nr, balance, cost, its, flags);
+        DomainSet set = structured
+                            ? DomainSet(nx, tp, nr, balance, cost, its, flags)
+                            : DomainSet(mesh.c_str(), nr, balance, cost, its, flags);
         Domain origin(set, 0);
         const int ranks = tp * tp * tp;
-        if (!quiet)
-            std::printf("Running until t=%f, Problem size=%dx%dx%d\n", 1.0e-2, nx * tp, nx * tp,
-                        nx * tp);
+        // zones of one domain: nx^3, or the mesh's element count
+        const double zones = structured ? (double)nx * nx * nx : (double)origin.numElem();
+        if (!quiet) {
+            if (structured)
+                std::printf("Running until t=%f, Problem size=%dx%dx%d\n", 1.0e-2, nx * tp,
+                            nx * tp, nx * tp);
+            else
+                std::printf("Running until t=%f, Problem size=%d \n", 1.0e-2, origin.numElem());
+        }
         // halo-exchange setup before the timed loop, as the reference sets up
         // its comm backend before it: the staged message tables and the
         // captured cycle graph (lulesh_step with 0 cycles builds both)
@@ -162,20 +183,23 @@ int main(int argc, char *argv[])
         cudaMemGetInfo(&free_mem, &total_mem);
         std::printf("   Used Memory         =  %8.4f Mb\n", (total_mem - free_mem) / (1024. * 1024.));
         const int cyc = s.cycle;
-        const double grind1 = ((elapsed * 1e6) / cyc) / ((double)nx * nx * nx);
-        const double grind2 = ((elapsed * 1e6) / cyc) / ((double)nx * nx * nx * ranks);
+        const double grind1 = ((elapsed * 1e6) / cyc) / zones;
+        const double grind2 = ((elapsed * 1e6) / cyc) / (zones * ranks);
         double e0 = 0.0, ma = 0.0, ta = 0.0, mr = 0.0;
         check(lulesh_origin_energy(set.get(), 0, &e0), "energy");
-        check(lulesh_symmetry(set.get(), 0, &ma, &ta, &mr), "symmetry");
-        std::printf("Run completed:  \n");
-        std::printf("   Problem size        =  %i \n", nx);
-        std::printf("   MPI tasks           =  %i \n", ranks);
-        std::printf("   Iteration count     =  %i \n", cyc);
-        std::printf("   Final Origin Energy = %12.6e \n", e0);
-        std::printf("   Testing Plane 0 of Energy Array on rank 0:\n");
-        std::printf("        MaxAbsDiff   = %12.6e\n", ma);
-        std::printf("        TotalAbsDiff = %12.6e\n", ta);
-        std::printf("        MaxRelDiff   = %12.6e\n\n", mr);
+        if (structured) {
+            // the reference prints this block for -s runs only
+            check(lulesh_symmetry(set.get(), 0, &ma, &ta, &mr), "symmetry");
+            std::printf("Run completed:  \n");
+            std::printf("   Problem size        =  %i \n", nx);
+            std::printf("   MPI tasks           =  %i \n", ranks);
+            std::printf("   Iteration count     =  %i \n", cyc);
+            std::printf("   Final Origin Energy = %12.6e \n", e0);
+            std::printf("   Testing Plane 0 of Energy Array on rank 0:\n");
+            std::printf("        MaxAbsDiff   = %12.6e\n", ma);
+            std::printf("        TotalAbsDiff = %12.6e\n", ta);
+            std::printf("        MaxRelDiff   = %12.6e\n\n", mr);
+        }
         std::printf("\nElapsed time         = %10.2f (s)\n", elapsed);
         std::printf("Grind time (us/z/c)  = %10.8g (per dom)  (%10.8g overall)\n", grind1, grind2);
         // the reference prints 1000/grind (zones per ms), kept for its parsers
@@ -201,7 +225,7 @@ int main(int argc, char *argv[])
         }
     } catch (const Error &e) {
         std::fprintf(stderr, "%s\n", e.what());
-        return e.status == LULESH_INVALID_ARG ? LFileError : 1;
+        return (e.status == LULESH_INVALID_ARG || e.status == LULESH_FILE_ERROR) ? LFileError : 1;
     }
     return 0;
 }

@@ -113,13 +113,26 @@ static int create_common(lulesh_set *s, const std::vector<DomPlace> &place, int 
     s->ndom = (int)place.size();
     const bool mixed = (s->flags & LULESH_FLAG_MIXED) != 0;
 
-    // arena
+    // arena (an lmesh domain is read first: the file gives its sizes)
     size_t total = 0;
     std::vector<long> commd(s->ndom);
-    for (int d = 0; d < s->ndom; ++d) {
-        const lulesh_job &j = s->jobs[place[d].job];
-        commd[d] = comm_buffer_doubles(j.nx, place[d].tp);
-        total += domain_bytes(sizes_of(j.nx, j.numReg, commd[d]), mixed);
+    HostDomain mesh;
+    if (s->unstructured) {
+        const lulesh_job &j = s->jobs[0];
+        std::string err;
+        if (!build_domain_lmesh(mesh, s->mesh_path.c_str(), j.numReg, j.balance, j.cost,
+                                &err)) {
+            set_error(err);
+            return LULESH_FILE_ERROR;
+        }
+        commd[0] = 0;
+        total = domain_bytes(sizes_of(mesh, 0), mixed);
+    } else {
+        for (int d = 0; d < s->ndom; ++d) {
+            const lulesh_job &j = s->jobs[place[d].job];
+            commd[d] = comm_buffer_doubles(j.nx, place[d].tp);
+            total += domain_bytes(sizes_of(j.nx, j.numReg, commd[d]), mixed);
+        }
     }
     s->arena_bytes = total;
     LCHECK(cudaMalloc(&s->arena, total));
@@ -137,7 +150,9 @@ static int create_common(lulesh_set *s, const std::vector<DomPlace> &place, int 
         const DomPlace &pl = place[d];
         const lulesh_job &j = s->jobs[pl.job];
         HostDomain h;
-        if (pl.tp == 1 && !(s->flags & LULESH_FLAG_HOST_SETUP))
+        if (s->unstructured)
+            h = std::move(mesh);
+        else if (pl.tp == 1 && !(s->flags & LULESH_FLAG_HOST_SETUP))
             build_domain_light(h, j.nx, j.numReg, j.balance, j.cost);
         else
             build_domain(h, j.nx, pl.tp, pl.col, pl.row, pl.plane, pl.rank, j.numReg, j.balance,
@@ -191,7 +206,7 @@ static int create_common(lulesh_set *s, const std::vector<DomPlace> &place, int 
 
 void launch_force_fp64(lulesh_set *s, cudaStream_t st)
 {
-    launch_force(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb);
+    launch_force(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb, s->unstructured);
 }
 
 int enqueue_cycle(lulesh_set *s)
@@ -207,15 +222,17 @@ int enqueue_cycle(lulesh_set *s)
     if (mixed)
         launch_nodal_mixed(s->args(s->node_blocks), s->n_node_blocks, s->P, s->dcorner32, st);
     else
-        launch_nodal(s->args(s->node_blocks), s->n_node_blocks, s->P, st, s->nb);
+        launch_nodal(s->args(s->node_blocks), s->n_node_blocks, s->P, st, s->nb,
+                         s->unstructured);
     if (s->tp > 1) launch_posvel_sync(s->args(s->node_blocks), s->n_node_blocks, st);
     if (mixed)
         launch_kinematics_mixed(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st);
     else
-        launch_kinematics(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb);
+        launch_kinematics(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb,
+                              s->unstructured);
     if (s->tp > 1 && s->n_ghost_blocks > 0)
         launch_monoq_ghost(s->args(s->ghost_blocks), s->n_ghost_blocks, st);
-    launch_eos(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb);
+    launch_eos(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb, s->unstructured);
     return cuda_status(cudaGetLastError(), "cycle launch");
 }
 
@@ -380,7 +397,12 @@ static bool field_of(const lulesh_set *s, int d, const char *name, FieldRef *out
 {
     const DomDev &D = s->hdoms[d];
     const size_t E = D.numElem, N = D.numNode, Ep = D.Ep, A = D.allElem;
-    const size_t en2 = (size_t)D.en * D.en, nr = D.numReg;
+    // symmetry sets: en^2 on -s meshes, the largest set of an lmesh
+    const size_t en2 =
+        D.unstructured
+            ? (size_t)std::max(1, std::max(D.numSymmX, std::max(D.numSymmY, D.numSymmZ)))
+            : (size_t)D.en * D.en;
+    const size_t nr = D.numReg;
     struct Row {
         const char *n;
         void *p;
@@ -519,6 +541,38 @@ int lulesh_create_batch(const lulesh_job *jobs, int njobs, int flags, int device
     std::vector<DomPlace> place;
     for (int j = 0; j < njobs; ++j) place.push_back(DomPlace{j, 1, 0, 0, 0, 0});
     int st = create_common(s, place, device);
+    if (st != LULESH_OK) {
+        lulesh_destroy(s);
+        return st;
+    }
+    *out = s;
+    return LULESH_OK;
+}
+
+int lulesh_create_from_mesh(const char *path, const lulesh_job *job, int flags, int device,
+                            lulesh_set **out)
+{
+    if (!path || !job || !out) {
+        set_error("lulesh_create_from_mesh: bad arguments");
+        return LULESH_INVALID_ARG;
+    }
+    *out = nullptr;
+    lulesh_job j = *job;
+    j.nx = 1;  // the mesh file gives the sizes
+    int st = validate_job(j);
+    if (st != LULESH_OK) return st;
+    if (flags & (LULESH_FLAG_COMM_STAGED | LULESH_FLAG_MIXED)) {
+        set_error("unstructured meshes run as one FP64 domain");
+        return LULESH_INVALID_ARG;
+    }
+    lulesh_set *s = new lulesh_set;
+    s->flags = flags;
+    s->tp = 1;
+    s->njobs = 1;
+    s->jobs.assign(1, j);
+    s->mesh_path = path;
+    s->unstructured = true;
+    st = create_common(s, {DomPlace{0, 1, 0, 0, 0, 0}}, device);
     if (st != LULESH_OK) {
         lulesh_destroy(s);
         return st;
@@ -679,19 +733,21 @@ int lulesh_profile_phases(lulesh_set *s, int ncycles, double *ms_out, int *nphas
         if (mixed)
             launch_nodal_mixed(s->args(s->node_blocks), s->n_node_blocks, s->P, s->dcorner32, st);
         else
-            launch_nodal(s->args(s->node_blocks), s->n_node_blocks, s->P, st, s->nb);
+            launch_nodal(s->args(s->node_blocks), s->n_node_blocks, s->P, st, s->nb,
+                         s->unstructured);
         LCHECK(cudaEventRecord(ev[3], st));
         if (s->tp > 1) launch_posvel_sync(s->args(s->node_blocks), s->n_node_blocks, st);
         LCHECK(cudaEventRecord(ev[4], st));
         if (mixed)
             launch_kinematics_mixed(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st);
         else
-            launch_kinematics(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb);
+            launch_kinematics(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb,
+                              s->unstructured);
         LCHECK(cudaEventRecord(ev[5], st));
         if (s->tp > 1 && s->n_ghost_blocks > 0)
             launch_monoq_ghost(s->args(s->ghost_blocks), s->n_ghost_blocks, st);
         LCHECK(cudaEventRecord(ev[6], st));
-        launch_eos(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb);
+        launch_eos(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb, s->unstructured);
         LCHECK(cudaEventRecord(ev[7], st));
         LCHECK(cudaEventSynchronize(ev[7]));
         for (int k = 0; k < np; ++k) {
@@ -723,7 +779,7 @@ int lulesh_origin_energy(lulesh_set *s, int job, double *energy)
     if (!s || !energy || job < 0 || job >= s->njobs) return LULESH_INVALID_ARG;
     const DomDev &D = s->hdoms[s->job_origin[job]];
     LCHECK(cudaStreamSynchronize(s->stream));
-    LCHECK(cudaMemcpy(energy, D.e, sizeof(double), cudaMemcpyDeviceToHost));
+    LCHECK(cudaMemcpy(energy, D.e + D.octant, sizeof(double), cudaMemcpyDeviceToHost));
     return LULESH_OK;
 }
 
@@ -731,6 +787,10 @@ int lulesh_symmetry(lulesh_set *s, int job, double *max_abs, double *total_abs, 
 {
     if (!s || job < 0 || job >= s->njobs) return LULESH_INVALID_ARG;
     const DomDev &D = s->hdoms[s->job_origin[job]];
+    if (D.unstructured) {
+        set_error("the plane-0 symmetry check needs a structured (-s) mesh");
+        return LULESH_INVALID_ARG;
+    }
     const int nx = D.nx;
     std::vector<double> e((size_t)nx * nx);
     LCHECK(cudaStreamSynchronize(s->stream));

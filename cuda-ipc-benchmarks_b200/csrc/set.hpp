@@ -18,6 +18,9 @@ struct lulesh_set {
     int flags = 0;
     lulesh::Params P{};
     int tp = 1;  // subdomains per axis of each job (1 for batches)
+    // one unstructured domain read from this lmesh file (empty: -s meshes)
+    std::string mesh_path;
+    bool unstructured = false;
     int ndom = 0, njobs = 0;
 
     // per-domain metadata kept on the host

@@ -27,7 +27,8 @@ namespace lulesh {
 
 static bool shapes_fixed(const lulesh_set *s)
 {
-    return s->tp > 1 || (s->flags & (LULESH_FLAG_COMM_STAGED | LULESH_FLAG_MIXED)) != 0;
+    return s->tp > 1 || s->unstructured ||
+           (s->flags & (LULESH_FLAG_COMM_STAGED | LULESH_FLAG_MIXED)) != 0;
 }
 
 static int apply(lulesh_set *s, const lulesh_tuning &t)

@@ -51,7 +51,7 @@ INT_FIELDS = {
 
 # every symbol include/lulesh_b200.h declares
 EXPORTED = [
-    "lulesh_create", "lulesh_create_batch", "lulesh_destroy",
+    "lulesh_create", "lulesh_create_batch", "lulesh_create_from_mesh", "lulesh_destroy",
     "lulesh_footprint_bytes", "lulesh_set_stream", "lulesh_lagrange_leapfrog",
     "lulesh_step", "lulesh_run", "lulesh_host_cycle", "lulesh_sync",
     "lulesh_num_jobs", "lulesh_num_domains", "lulesh_job_state_get",
@@ -136,6 +136,8 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
     sig = {
         "lulesh_create": (ip, [ctypes.POINTER(Job), ip, ip, ip, ctypes.POINTER(vp)]),
         "lulesh_create_batch": (ip, [ctypes.POINTER(Job), ip, ip, ip, ctypes.POINTER(vp)]),
+        "lulesh_create_from_mesh": (ip, [ctypes.c_char_p, ctypes.POINTER(Job), ip, ip,
+                                         ctypes.POINTER(vp)]),
         "lulesh_destroy": (ip, [vp]),
         "lulesh_footprint_bytes": (ctypes.c_size_t, [ctypes.POINTER(Job), ip, ip]),
         "lulesh_set_stream": (ip, [vp, vp]),
@@ -242,6 +244,19 @@ class LuleshSet:
         h = ctypes.c_void_p()
         _check(lib, lib.lulesh_create_batch(arr, len(jobs), flags, device, ctypes.byref(h)),
                "lulesh_create_batch")
+        return cls(_handle=h)
+
+    @classmethod
+    def from_mesh(cls, path: str, numReg: int = 11, balance: int = 1, cost: int = 1,
+                  its: int = -1, flags: int = 0, device: int = -1) -> "LuleshSet":
+        """One unstructured domain read from an lmesh file (the reference's
+        `-u file.lmesh`); FILE_ERROR for a missing or malformed file."""
+        lib = load_library()
+        job = JobSpec(1, numReg, balance, cost, its).c()
+        h = ctypes.c_void_p()
+        _check(lib, lib.lulesh_create_from_mesh(str(path).encode(), ctypes.byref(job), flags,
+                                                device, ctypes.byref(h)),
+               "lulesh_create_from_mesh")
         return cls(_handle=h)
 
     # -- lifetime

@@ -136,6 +136,18 @@ int lulesh_create(const lulesh_job *job, int tp, int flags, int device,
 int lulesh_create_batch(const lulesh_job *jobs, int njobs, int flags,
                         int device, lulesh_set **out);
 
+/* Replaces NewDomain's unstructured branch (lulesh.cu:855-1052, the `-u
+ * file.lmesh` run): one FP64 domain read from an lmesh file ("E N" header,
+ * N coordinate lines, E lines of 8 node ids, E lines of 6 face links, then
+ * the symmX/Y/Z and free-surface node sets, each a count followed by ids).
+ * job->nx is ignored; numReg/balance/cost/its keep their meaning.  The
+ * energy deposit goes to the element whose three minus faces carry
+ * symmetry, and free-surface faces carry the *_FREE boundary bits.
+ * Returns LULESH_FILE_ERROR for an unreadable or malformed file, and
+ * LULESH_INVALID_ARG with LULESH_FLAG_COMM_STAGED or LULESH_FLAG_MIXED. */
+int lulesh_create_from_mesh(const char *path, const lulesh_job *job,
+                            int flags, int device, lulesh_set **out);
+
 /* Frees the arena, graphs and streams (the reference's teardown,
  * lulesh.cu:4904-4944, minus MPI). */
 int lulesh_destroy(lulesh_set *set);

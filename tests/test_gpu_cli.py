@@ -62,3 +62,21 @@ def test_errors_map_to_reference_exit_codes(tmp_path):
     assert r.returncode != 0
     r = _run("-s", "8", "-i", "5", "-q", "--no-xyz", cwd=tmp_path)
     assert r.returncode == 0 and r.stdout == ""
+
+
+def test_unstructured_form(tmp_path):
+    """-u FILE x ITERS: the reference's unstructured report (problem size =
+    element count, no plane-0 block), and the -s 45 cube as an lmesh file
+    gives the -s 45 energy."""
+    import lmesh
+
+    p = tmp_path / "box45.lmesh"
+    lmesh.write(p, lmesh.box(45))
+    u = _run("-u", str(p), "x", "100", cwd=tmp_path)
+    s = _run("-s", "45", "x", "100", cwd=tmp_path)
+    assert u.returncode == 0 and s.returncode == 0, u.stdout + u.stderr
+    assert "Problem size=91125" in u.stdout
+    assert not _awk(u.stdout, "Final Origin Energy", 5)
+    full = [re.search(r"Origin energy, 17 digits = (\S+)", r.stdout).group(1) for r in (u, s)]
+    assert full[0] == full[1]
+    assert len(_awk(u.stdout, "FOM", 3)) == 1

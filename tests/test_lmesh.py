@@ -1,0 +1,51 @@
+"""The lmesh writer/reader (the reference's -u input format, lulesh.cu:855-1052):
+the cube it writes is the -s mesh of the oracle's BuildMesh restatement, and
+files round-trip exactly."""
+import numpy as np
+import pytest
+
+import lmesh
+
+
+@pytest.mark.parametrize("nx", [1, 3, 7])
+def test_box_is_the_structured_mesh(oracle_mod, nx):
+    m = lmesh.box(nx)
+    o = oracle_mod.Oracle(nx)
+    try:
+        E, N = m.num_elem, m.num_node
+        Ep = int(o.scalar("padded_numElem"))
+        nl = o.field("nodelist").reshape(8, Ep)[:, :E].T
+        assert (m.nodelist == nl).all()
+        for k, name in enumerate(["lxim", "lxip", "letam", "letap", "lzetam", "lzetap"]):
+            assert (m.links[:, k] == o.field(name)[:E]).all(), name
+        for k, c in enumerate("xyz"):
+            assert (m.xyz[:, k] == o.field(c)[:N]).all()
+        for k, name in enumerate(["symmX", "symmY", "symmZ"]):
+            n = int(o.scalar("numSymm" + "XYZ"[k]))
+            assert sorted(o.field(name)[:n]) == list(m.symm[k])
+    finally:
+        o.close()
+
+
+def test_round_trip(tmp_path):
+    m = lmesh.box(4)
+    p = tmp_path / "b.lmesh"
+    lmesh.write(p, m)
+    r = lmesh.read(p)
+    assert (r.xyz == m.xyz).all()
+    assert (r.nodelist == m.nodelist).all() and (r.links == m.links).all()
+    assert all((a == b).all() for a, b in zip(r.symm, m.symm))
+    assert (r.free == m.free).all()
+
+
+def test_renumber_keeps_geometry():
+    m = lmesh.box(3)
+    rng = np.random.default_rng(7)
+    npm = rng.permutation(m.num_node)
+    epm = rng.permutation(m.num_elem)
+    r = lmesh.renumber(m, npm, epm)
+    # element epm[z] has the coordinates of element z, corner by corner
+    assert (r.xyz[r.nodelist[epm]] == m.xyz[m.nodelist]).all()
+    # face neighbours map the same way
+    assert (r.links[epm] == epm[m.links]).all()
+    assert sorted(r.free) == sorted(npm[m.free])
