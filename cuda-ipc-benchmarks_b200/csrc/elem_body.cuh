@@ -81,13 +81,14 @@ __device__ __forceinline__ void elem_nodes(const DomDev &D, int el, int n[8])
 }
 
 // CalcVolumeForceForElems_kernel (lulesh.cu:2080-2259) after the node
-// gathers: stress + FB hourglass corner forces of element `elem`, written
-// to the corner arrays at elem + Ep * corner.  The velocities are fetched
+// gathers: stress + FB hourglass corner forces of element `elem`, handed
+// to store(k, fx, fy, fz) corner by corner.  The velocities are fetched
 // from `vel` only when HG (hourglass coefficient > 0).
-template <bool HG, class Vel>
-__device__ __forceinline__ void force_elem(const DomDev &D, TimeCtl &T, const Params &P, int elem,
-                                           const double (&xn)[8], const double (&yn)[8],
-                                           const double (&zn)[8], const Vel &vel)
+template <bool HG, class Vel, class Store>
+__device__ __forceinline__ void force_elem_to(const DomDev &D, TimeCtl &T, const Params &P,
+                                              int elem, const double (&xn)[8],
+                                              const double (&yn)[8], const double (&zn)[8],
+                                              const Vel &vel, const Store &store)
 {
     double dvdxn[8], dvdyn[8], dvdzn[8];
     double hgfx[8], hgfy[8], hgfz[8];
@@ -126,13 +127,29 @@ __device__ __forceinline__ void force_elem(const DomDev &D, TimeCtl &T, const Pa
         fb_hourglass_component(ydn, hourgam, coefficient, hgfy);
         fb_hourglass_component(zdn, hourgam, coefficient, hgfz);
     }
-    const int Ep = D.Ep;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        st_corner(D.fx_elem + elem + Ep * k, hgfx[k]);
-        st_corner(D.fy_elem + elem + Ep * k, hgfy[k]);
-        st_corner(D.fz_elem + elem + Ep * k, hgfz[k]);
+    for (int k = 0; k < 8; ++k) store(k, hgfx[k], hgfy[k], hgfz[k]);
+}
+
+// the corner arrays at elem + Ep * corner
+struct CornerStore {
+    const DomDev &D;
+    int elem;
+    __device__ __forceinline__ void operator()(int k, double fx, double fy, double fz) const
+    {
+        const int c = elem + D.Ep * k;
+        st_corner(D.fx_elem + c, fx);
+        st_corner(D.fy_elem + c, fy);
+        st_corner(D.fz_elem + c, fz);
     }
+};
+
+template <bool HG, class Vel>
+__device__ __forceinline__ void force_elem(const DomDev &D, TimeCtl &T, const Params &P, int elem,
+                                           const double (&xn)[8], const double (&yn)[8],
+                                           const double (&zn)[8], const Vel &vel)
+{
+    force_elem_to<HG>(D, T, P, elem, xn, yn, zn, vel, CornerStore{D, elem});
 }
 
 // CalcKinematicsAndMonotonicQGradient_kernel (lulesh.cu:3343-3507) after

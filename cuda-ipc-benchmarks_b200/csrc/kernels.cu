@@ -212,6 +212,48 @@ __device__ __forceinline__ void gather_corners(const DomDev *doms, const DomDev 
     }
 }
 
+// CalcAccelerationForNodes (lulesh.cu:2926-2939), the symmetry-plane zeroing
+// of ApplyAccelerationBoundaryConditionsForNodes (bc bits 0/1/2 zero the
+// x/y/z acceleration) and CalcPositionAndVelocityForNodes (lulesh.cu:
+// 2999-3028) for node i with the summed force (fx, fy, fz)
+__device__ __forceinline__ void advance_node(const DomDev &D, const TimeCtl &T, const Params &P,
+                                             int i, int bc, double fx, double fy, double fz,
+                                             int materialize, bool write_f)
+{
+    const double one_over_nMass = 1. / D.nodalMass[i];
+    double xdd = fx * one_over_nMass;
+    double ydd = fy * one_over_nMass;
+    double zdd = fz * one_over_nMass;
+    if (bc & 1) xdd = 0.0;
+    if (bc & 2) ydd = 0.0;
+    if (bc & 4) zdd = 0.0;
+
+    const double dt = T.deltatime;
+    const double u_cut = P.u_cut;
+    double xdtmp = D.xd[i] + xdd * dt;
+    double ydtmp = D.yd[i] + ydd * dt;
+    double zdtmp = D.zd[i] + zdd * dt;
+    if (fabs(xdtmp) < u_cut) xdtmp = 0.0;
+    if (fabs(ydtmp) < u_cut) ydtmp = 0.0;
+    if (fabs(zdtmp) < u_cut) zdtmp = 0.0;
+    D.x[i] += xdtmp * dt;
+    D.y[i] += ydtmp * dt;
+    D.z[i] += zdtmp * dt;
+    D.xd[i] = xdtmp;
+    D.yd[i] = ydtmp;
+    D.zd[i] = zdtmp;
+    if (materialize) {
+        if (write_f) {
+            D.fx[i] = fx;
+            D.fy[i] = fy;
+            D.fz[i] = fz;
+        }
+        D.xdd[i] = xdd;
+        D.ydd[i] = ydd;
+        D.zdd[i] = zdd;
+    }
+}
+
 // MODE 0: gather every corner (neighbour subdomains included) and update
 //         the node: the fused form of the SBN exchange + node update.
 // MODE 1: AddNodeForcesFromElems over this domain's own corners only,
@@ -263,50 +305,16 @@ __global__ void __launch_bounds__(BS, min_blocks(kNodalMinBlocks, BS)) k_nodal(S
         fz = D.fz[i];
     }
 
-    // CalcAccelerationForNodes_kernel, lulesh.cu:2926-2939
-    const double one_over_nMass = 1. / D.nodalMass[i];
-    double xdd = fx * one_over_nMass;
-    double ydd = fy * one_over_nMass;
-    double zdd = fz * one_over_nMass;
     // ApplyAccelerationBoundaryConditionsForNodes: symmetry planes are the
     // px/py/pz == 0 node sets of the domains at the mesh origin faces (an
     // unstructured mesh lists its symmetry nodes: nodeBC bits)
-    if (U) {
-        const int m = D.nodeBC[i];
-        if (m & 1) xdd = 0.0;
-        if (m & 2) ydd = 0.0;
-        if (m & 4) zdd = 0.0;
-    } else {
-        if (D.col == 0 && px == 0) xdd = 0.0;
-        if (D.row == 0 && py == 0) ydd = 0.0;
-        if (D.plane == 0 && pz == 0) zdd = 0.0;
-    }
-
-    // CalcPositionAndVelocityForNodes_kernel, lulesh.cu:2999-3028
-    const double dt = T.deltatime;
-    const double u_cut = P.u_cut;
-    double xdtmp = D.xd[i] + xdd * dt;
-    double ydtmp = D.yd[i] + ydd * dt;
-    double zdtmp = D.zd[i] + zdd * dt;
-    if (fabs(xdtmp) < u_cut) xdtmp = 0.0;
-    if (fabs(ydtmp) < u_cut) ydtmp = 0.0;
-    if (fabs(zdtmp) < u_cut) zdtmp = 0.0;
-    D.x[i] += xdtmp * dt;
-    D.y[i] += ydtmp * dt;
-    D.z[i] += zdtmp * dt;
-    D.xd[i] = xdtmp;
-    D.yd[i] = ydtmp;
-    D.zd[i] = zdtmp;
-    if (a.materialize) {
-        if (MODE == 0) {
-            D.fx[i] = fx;
-            D.fy[i] = fy;
-            D.fz[i] = fz;
-        }
-        D.xdd[i] = xdd;
-        D.ydd[i] = ydd;
-        D.zdd[i] = zdd;
-    }
+    int bc;
+    if (U)
+        bc = D.nodeBC[i];
+    else
+        bc = (D.col == 0 && px == 0 ? 1 : 0) | (D.row == 0 && py == 0 ? 2 : 0) |
+             (D.plane == 0 && pz == 0 ? 4 : 0);
+    advance_node(D, T, P, i, bc, fx, fy, fz, a.materialize, MODE == 0);
 }
 
 void launch_nodal(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs, bool u)
