@@ -622,6 +622,21 @@ int lulesh_lagrange_leapfrog(lulesh_set *s) { return lulesh_step(s, 1); }
 int lulesh_step(lulesh_set *s, int ncycles)
 {
     if (!s || ncycles < 0) return LULESH_INVALID_ARG;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    LCHECK(cudaStreamIsCapturing(s->stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone) {
+        // the caller is capturing the set's stream into a graph of its own:
+        // the cycle's kernels become nodes of that graph
+        if (!s->graph_ready) {
+            set_error("lulesh_step: call lulesh_step(set, 0) before capturing the set's stream");
+            return LULESH_INVALID_ARG;
+        }
+        for (int i = 0; i < ncycles; ++i) {
+            const int est = enqueue_cycle(s);
+            if (est != LULESH_OK) return est;
+        }
+        return LULESH_OK;
+    }
     int st = ensure_graph(s);
     if (st != LULESH_OK) return st;
     if (s->graph_cycles > 1 && ncycles >= s->graph_cycles) {

@@ -167,7 +167,11 @@ int lulesh_set_stream(lulesh_set *set, void *stream);
  * with TimeIncrement moved onto the device).  Jobs that are done skip. */
 int lulesh_lagrange_leapfrog(lulesh_set *set);
 
-/* `ncycles` such cycles, asynchronously. */
+/* `ncycles` such cycles, asynchronously.  On a stream the caller is
+ * capturing into its own CUDA graph, the cycles' kernels are enqueued one
+ * by one and become nodes of that graph; make one lulesh_step(set, 0) call
+ * before the capture (it prepares the set outside the capture), or the
+ * call returns LULESH_INVALID_ARG.  ncycles = 0 only prepares. */
 int lulesh_step(lulesh_set *set, int ncycles);
 
 /* The whole run in one CUDA graph launch: a WHILE conditional node repeats
