@@ -93,6 +93,21 @@ def renumber(m: LMesh, node_perm: np.ndarray | None = None,
     return LMesh(xyz, nodelist, links, symm, free)
 
 
+def warp(m: LMesh, amp: float = 0.05) -> LMesh:
+    """A curvilinear copy of a box mesh: every node moves by a smooth
+    displacement that vanishes on the planes x, y, z = 0 and = max, so the
+    symmetry planes and the free surface stay where they were."""
+    lo, hi = m.xyz.min(axis=0), m.xyz.max(axis=0)
+    u = (m.xyz - lo) / (hi - lo)  # 0..1 per axis
+    bump = np.sin(np.pi * u)      # 0 on both end planes
+    xyz = m.xyz.copy()
+    for a in range(3):
+        b, c = (a + 1) % 3, (a + 2) % 3
+        xyz[:, a] += amp * (hi[a] - lo[a]) * bump[:, a] * np.sin(2 * np.pi * u[:, b]) * \
+            np.cos(np.pi * u[:, c])
+    return LMesh(xyz, m.nodelist.copy(), m.links.copy(), m.symm, m.free)
+
+
 def write(path, m: LMesh) -> None:
     with open(path, "w") as f:
         f.write(f"{m.num_elem} {m.num_node}\n")

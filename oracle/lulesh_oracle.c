@@ -19,6 +19,7 @@
 
 #include <limits.h>
 #include <math.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -78,6 +79,8 @@ struct OracleDomain {
     double time, deltatime, dtcourant, dthydro, initial_deltatime;
     int cycle;
     int bad_vol, bad_q;
+    /* element holding the energy deposit (0 on -s meshes) */
+    int octantCorner;
 };
 
 static void *zalloc(size_t n) { return calloc(n ? n : 1, 1); }
@@ -515,6 +518,34 @@ static void create_regions(OracleDomain *d, int nr, int balance)
     }
 }
 
+/* node -> corner CSR, lulesh.cu:1054-1106 (outer j, inner element) */
+static void corner_csr(OracleDomain *d)
+{
+    const int E = d->numElem, N = d->numNode, Ep = d->Ep;
+    d->nodeElemCount = ZI(N);
+    d->nodeElemStart = ZI(N);
+    for (int i = 0; i < E; ++i)
+        for (int j = 0; j < 8; ++j) d->nodeElemCount[d->nodelist[j * Ep + i]]++;
+    d->nodeElemStart[0] = 0;
+    for (int i = 1; i < N; ++i)
+        d->nodeElemStart[i] = d->nodeElemStart[i - 1] + d->nodeElemCount[i - 1];
+    d->cornerListLen = d->nodeElemStart[N - 1] + d->nodeElemCount[N - 1];
+    d->nodeElemCornerList = ZI(d->cornerListLen);
+    for (int i = 0; i < N; ++i) d->nodeElemCount[i] = 0;
+    for (int j = 0; j < 8; ++j)
+        for (int i = 0; i < E; ++i) {
+            int m = d->nodelist[Ep * j + i];
+            int off = d->nodeElemStart[m] + d->nodeElemCount[m];
+            d->nodeElemCornerList[off] = Ep * j + i;
+            d->nodeElemCount[m]++;
+        }
+    d->matElemlist = ZI(E);
+    for (int i = 0; i < E; ++i) d->matElemlist[i] = i;
+}
+
+static void set_params(OracleDomain *d);
+static void masses(OracleDomain *d);
+
 OracleDomain *oracle_create(int nx, int numReg, int balance, int cost,
                             int tp, int col, int row, int plane, int rank)
 {
@@ -692,28 +723,26 @@ OracleDomain *oracle_create(int nx, int numReg, int balance, int cost,
         }
     }
 
-    /* node -> corner CSR, lulesh.cu:1054-1106 (outer j, inner element) */
-    d->nodeElemCount = ZI(N);
-    d->nodeElemStart = ZI(N);
-    for (int i = 0; i < E; ++i)
-        for (int j = 0; j < 8; ++j) d->nodeElemCount[d->nodelist[j * Ep + i]]++;
-    d->nodeElemStart[0] = 0;
-    for (int i = 1; i < N; ++i)
-        d->nodeElemStart[i] = d->nodeElemStart[i - 1] + d->nodeElemCount[i - 1];
-    d->cornerListLen = d->nodeElemStart[N - 1] + d->nodeElemCount[N - 1];
-    d->nodeElemCornerList = ZI(d->cornerListLen);
-    for (int i = 0; i < N; ++i) d->nodeElemCount[i] = 0;
-    for (int j = 0; j < 8; ++j)
-        for (int i = 0; i < E; ++i) {
-            int m = d->nodelist[Ep * j + i];
-            int off = d->nodeElemStart[m] + d->nodeElemCount[m];
-            d->nodeElemCornerList[off] = Ep * j + i;
-            d->nodeElemCount[m]++;
-        }
-    d->matElemlist = ZI(E);
-    for (int i = 0; i < E; ++i) d->matElemlist[i] = i;
+    corner_csr(d);
+    set_params(d);
+    /* volo, elemMass, nodalMass, lulesh.cu:1165-1187 */
+    masses(d);
 
-    /* parameters, lulesh.cu:1120-1158 */
+    /* energy deposit and initial dt, lulesh.cu:1189-1205 */
+    const double ebase = 3.948746e+7;
+    double scale = (nx * tp) / 45.0;
+    double einit = ebase * scale * scale * scale;
+    if (row + col + plane == 0) d->e[0] = einit;
+    d->deltatime = (.5 * cbrt(d->volo[0])) / sqrt(2 * einit);
+    d->initial_deltatime = d->deltatime;
+
+    create_regions(d, numReg, balance);
+    return d;
+}
+
+/* parameters, lulesh.cu:1120-1158 */
+static void set_params(OracleDomain *d)
+{
     d->bad_vol = -1;
     d->bad_q = -1;
     d->dthydro = 1e20;
@@ -744,8 +773,12 @@ OracleDomain *oracle_create(int nx, int numReg, int balance, int cost,
     d->eosvmax = 1.0e+9;
     d->eosvmin = 1.0e-9;
     d->refdens = 1.0;
+}
 
-    /* volo, elemMass, nodalMass, lulesh.cu:1165-1187 */
+/* volo, elemMass, nodalMass, lulesh.cu:1165-1187 */
+static void masses(OracleDomain *d)
+{
+    const int E = d->numElem, Ep = d->Ep;
     for (int i = 0; i < E; ++i) {
         double xl[8], yl[8], zl[8];
         for (int k = 0; k < 8; ++k) {
@@ -760,15 +793,159 @@ OracleDomain *oracle_create(int nx, int numReg, int balance, int cost,
         for (int k = 0; k < 8; ++k)
             d->nodalMass[d->nodelist[k * Ep + i]] += vol / 8.0;
     }
+}
 
-    /* energy deposit and initial dt, lulesh.cu:1189-1205 */
-    const double ebase = 3.948746e+7;
-    double scale = (nx * tp) / 45.0;
-    double einit = ebase * scale * scale * scale;
-    if (row + col + plane == 0) d->e[0] = einit;
-    d->deltatime = (.5 * cbrt(d->volo[0])) / sqrt(2 * einit);
+/* lmesh reader: whitespace-separated ints and doubles, 0 at a read failure */
+static int rd_int(FILE *f, int *ok)
+{
+    int v = 0;
+    if (*ok && fscanf(f, "%d", &v) != 1) *ok = 0;
+    return v;
+}
+
+static double rd_real(FILE *f, int *ok)
+{
+    double v = 0.0;
+    if (*ok && fscanf(f, "%lf", &v) != 1) *ok = 0;
+    return v;
+}
+
+/* OR `bits` of the faces whose four nodes are all marked (the face tests of
+ * lulesh.cu:1001-1012, 1035-1045); order zeta-, zeta+, eta-, eta+, xi-, xi+ */
+static void mark_faces(OracleDomain *d, const char *mark, const int bits[6])
+{
+    static const int face[6] = {0x0f, 0xf0, 0x33, 0xcc, 0x99, 0x66};
+    for (int z = 0; z < d->numElem; ++z) {
+        int mask = 0;
+        for (int k = 0; k < 8; ++k)
+            if (mark[d->nodelist[k * d->Ep + z]]) mask |= 1 << k;
+        for (int f = 0; f < 6; ++f)
+            if ((mask & face[f]) == face[f]) d->elemBC[z] |= bits[f];
+    }
+}
+
+OracleDomain *oracle_create_lmesh(const char *path, int numReg, int balance, int cost)
+{
+    if (!path || numReg < 1) return NULL;
+    FILE *f = fopen(path, "r");
+    if (!f) return NULL;
+    int ok = 1;
+    const int E = rd_int(f, &ok), N = rd_int(f, &ok);
+    if (!ok || E < 1 || N < 8) {
+        fclose(f);
+        return NULL;
+    }
+    OracleDomain *d = (OracleDomain *)zalloc(sizeof(OracleDomain));
+    d->nx = 0;
+    d->tp = 1;
+    d->cost = cost;
+    d->numElem = E;
+    d->numNode = N;
+    d->Ep = ((E + 31) / 32) * 32;
+    d->allElem = E;
+    const int Ep = d->Ep;
+    d->e = ZD(E); d->p = ZD(E); d->q = ZD(E); d->ql = ZD(E); d->qq = ZD(E);
+    d->v = ZD(E); d->volo = ZD(E); d->delv = ZD(E); d->vdov = ZD(E);
+    d->arealg = ZD(E); d->ss = ZD(E); d->elemMass = ZD(E);
+    d->x = ZD(N); d->y = ZD(N); d->z = ZD(N);
+    d->xd = ZD(N); d->yd = ZD(N); d->zd = ZD(N);
+    d->xdd = ZD(N); d->ydd = ZD(N); d->zdd = ZD(N);
+    d->fx = ZD(N); d->fy = ZD(N); d->fz = ZD(N); d->nodalMass = ZD(N);
+    d->vnew = ZD(E);
+    d->delx_xi = ZD(E); d->delx_eta = ZD(E); d->delx_zeta = ZD(E);
+    d->delv_xi = ZD(E); d->delv_eta = ZD(E); d->delv_zeta = ZD(E);
+    d->fx_elem = ZD(8 * Ep); d->fy_elem = ZD(8 * Ep); d->fz_elem = ZD(8 * Ep);
+    for (int i = 0; i < E; ++i) d->v[i] = 1.0;
+
+    /* the -u branch of NewDomain, lulesh.cu:855-1052 */
+    for (int i = 0; i < N; ++i) {
+        d->x[i] = rd_real(f, &ok);
+        d->y[i] = rd_real(f, &ok);
+        d->z[i] = rd_real(f, &ok);
+    }
+    d->nodelist = ZI(8 * Ep);
+    for (int z = 0; z < E; ++z)
+        for (int k = 0; k < 8; ++k) {
+            int n = rd_int(f, &ok);
+            if (n < 0 || n >= N) ok = 0;
+            d->nodelist[k * Ep + z] = ok ? n : 0;
+        }
+    d->lxim = ZI(E); d->lxip = ZI(E); d->letam = ZI(E); d->letap = ZI(E);
+    d->lzetam = ZI(E); d->lzetap = ZI(E); d->elemBC = ZI(E);
+    int *links[6] = {d->lxim, d->lxip, d->letam, d->letap, d->lzetam, d->lzetap};
+    for (int z = 0; z < E; ++z)
+        for (int l = 0; l < 6; ++l) {
+            int v = rd_int(f, &ok);
+            if (v < 0 || v >= E) ok = 0;
+            links[l][z] = ok ? v : 0;
+        }
+    char *symm = (char *)zalloc((size_t)N), *freesurf = (char *)zalloc((size_t)N);
+    int *sets[3] = {NULL, NULL, NULL}, counts[3] = {0, 0, 0};
+    for (int a = 0; a < 3; ++a) {
+        int c = rd_int(f, &ok);
+        if (c < 0 || c > N) ok = 0;
+        counts[a] = ok ? c : 0;
+        sets[a] = ZI(counts[a]);
+        for (int k = 0; k < counts[a]; ++k) {
+            int n = rd_int(f, &ok);
+            if (n < 0 || n >= N) ok = 0;
+            sets[a][k] = ok ? n : 0;
+            if (ok) symm[n] = 1;
+        }
+    }
+    int nfree = rd_int(f, &ok);
+    if (nfree < 0 || nfree > N) ok = 0;
+    for (int k = 0; ok && k < nfree; ++k) {
+        int n = rd_int(f, &ok);
+        if (n < 0 || n >= N) ok = 0;
+        if (ok) freesurf[n] = 1;
+    }
+    fclose(f);
+    int len = 1;
+    for (int a = 0; a < 3; ++a) len = counts[a] > len ? counts[a] : len;
+    d->symmLen = len;
+    int **dst[3] = {&d->symmX, &d->symmY, &d->symmZ};
+    for (int a = 0; a < 3; ++a) {
+        *dst[a] = ZI(len);
+        memcpy(*dst[a], sets[a], sizeof(int) * (size_t)counts[a]);
+        free(sets[a]);
+    }
+    d->numSymmX = counts[0];
+    d->numSymmY = counts[1];
+    d->numSymmZ = counts[2];
+    if (!ok) {
+        free(symm);
+        free(freesurf);
+        oracle_destroy(d);
+        return NULL;
+    }
+    /* boundary masks: symmetry faces, then free-surface faces.  Deliberate
+     * difference: the reference tags free-surface faces with the *_SYMM
+     * bits (lulesh.cu:1039-1044); they get the *_FREE bits here. */
+    const int symm_bits[6] = {BC_ZETA_M_SYMM, BC_ZETA_P_SYMM, BC_ETA_M_SYMM,
+                              BC_ETA_P_SYMM, BC_XI_M_SYMM, BC_XI_P_SYMM};
+    const int free_bits[6] = {BC_ZETA_M_FREE, BC_ZETA_P_FREE, BC_ETA_M_FREE,
+                              BC_ETA_P_FREE, BC_XI_M_FREE, BC_XI_P_FREE};
+    mark_faces(d, symm, symm_bits);
+    d->octantCorner = 0;
+    for (int z = 0; z < E; ++z)
+        if (d->elemBC[z] == (BC_XI_M_SYMM | BC_ETA_M_SYMM | BC_ZETA_M_SYMM)) {
+            d->octantCorner = z;
+            break;
+        }
+    mark_faces(d, freesurf, free_bits);
+    free(symm);
+    free(freesurf);
+
+    corner_csr(d);
+    set_params(d);
+    masses(d);
+    /* deposit at the octant corner (lulesh.cu:1050); the shared setup's
+     * overwrite with einit(nx = 0) = 0 (lulesh.cu:1189-1205) is not kept */
+    const double einit = 3.948746e+7;
+    d->e[d->octantCorner] = einit;
+    d->deltatime = (.5 * cbrt(d->volo[d->octantCorner])) / sqrt(2 * einit);
     d->initial_deltatime = d->deltatime;
-
     create_regions(d, numReg, balance);
     return d;
 }
@@ -1354,7 +1531,7 @@ double oracle_scalar(OracleDomain *d, const char *name)
 
 void oracle_set_deltatime(OracleDomain *d, double dt) { d->deltatime = dt; }
 
-double oracle_origin_energy(OracleDomain *d) { return d->e[0]; }
+double oracle_origin_energy(OracleDomain *d) { return d->e[d->octantCorner]; }
 
 /* symmetry check of plane 0, lulesh.cu:4712-4736 */
 void oracle_symmetry(OracleDomain *d, double *max_abs, double *total_abs,

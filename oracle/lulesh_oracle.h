@@ -26,6 +26,13 @@ typedef struct OracleDomain OracleDomain;
  * A single domain is tp=1, col=row=plane=rank=0. */
 OracleDomain *oracle_create(int nx, int numReg, int balance, int cost,
                             int tp, int col, int row, int plane, int rank);
+/* One unstructured domain read from an lmesh file, as the -u branch of
+ * NewDomain reads it (lulesh.cu:855-1052), with the two corrections the
+ * product makes: free-surface faces carry the *_FREE bits, and the energy
+ * 3.948746e7 stays at the octant corner (the initial dt follows from that
+ * element's volume).  NULL for an unreadable or malformed file. */
+OracleDomain *oracle_create_lmesh(const char *path, int numReg, int balance,
+                                  int cost);
 void oracle_destroy(OracleDomain *d);
 
 /* One cycle: TimeIncrement then LagrangeLeapFrog (lulesh.cu:4438-4452,

@@ -43,6 +43,8 @@ def load() -> ctypes.CDLL:
     vp, ip, dp = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
     lib.oracle_create.restype = vp
     lib.oracle_create.argtypes = [ip] * 9
+    lib.oracle_create_lmesh.restype = vp
+    lib.oracle_create_lmesh.argtypes = [ctypes.c_char_p, ip, ip, ip]
     lib.oracle_destroy.argtypes = [vp]
     lib.oracle_step.restype = ip
     lib.oracle_step.argtypes = [vp]
@@ -72,6 +74,18 @@ class Oracle:
         if not self.h:
             raise ValueError("oracle_create rejected the arguments")
         self.nx = nx
+
+    @classmethod
+    def from_lmesh(cls, path: str, numReg: int = 11, balance: int = 1,
+                   cost: int = 1) -> "Oracle":
+        """The -u branch of NewDomain (lulesh.cu:855-1052) on an lmesh file."""
+        o = cls.__new__(cls)
+        o.lib = load()
+        o.h = o.lib.oracle_create_lmesh(str(path).encode(), numReg, balance, cost)
+        if not o.h:
+            raise ValueError(f"oracle_create_lmesh could not read {path}")
+        o.nx = 0
+        return o
 
     def close(self) -> None:
         if self.h:

@@ -57,6 +57,22 @@ def test_fields_match_oracle(lulesh, oracle_mod, nx, cycles, rtol):
             assert _close(gs.field(f), orc.field(f), rtol), f
 
 
+@pytest.mark.parametrize("nx", [1, 2, 3, 5])
+def test_small_meshes_full_run(lulesh, oracle_mod, nx):
+    """Edge sizes: a single element (every face on a boundary) up to -s 5,
+    run to t = 0.01; same cycle count, time and energies as the oracle."""
+    with lulesh.LuleshSet(nx=nx, its=-1) as gs:
+        orc = oracle_mod.Oracle(nx)
+        ost, ocyc = orc.run()
+        assert gs.run() == ost == lulesh.OK
+        st = gs.state()
+        assert st["cycle"] == ocyc and st["done"] == 1
+        assert rel(st["time"], orc.scalar("time")) < 1e-12
+        assert rel(gs.origin_energy(), orc.origin_energy()) < E_TOL
+        bad = _compare_state(gs, orc, 1e-9, ["e", "p", "q", "v", "x", "xd"])
+        assert not bad, bad
+
+
 def test_setup_matches_oracle(lulesh, oracle_mod):
     """Everything NewDomain builds (lulesh.cu:750-1221) is laid out as the
     reference lays it out: bit-exact for index data and the initial state."""

@@ -114,6 +114,61 @@ def test_element_renumbering(lulesh, tmp_path):
     assert np.abs(x_a - x_b).max() <= 1e-12
 
 
+def _compare(s, o, fields, E, N, rtol, atol=1e-14):
+    """Max difference relative to the field's largest magnitude; a field
+    that is still ~0 everywhere (delv after one cycle: the last bit of a
+    relative volume of 1) is held to `atol` instead."""
+    bad = []
+    for f in fields:
+        n = E if f in ELEM_FIELDS else N
+        g, r = s.field(f)[:n], o.field(f)[:n]
+        diff = float(np.max(np.abs(g - r)))
+        scale = float(max(np.max(np.abs(r)), np.max(np.abs(g))))
+        if diff > rtol * scale and diff > atol:
+            bad.append(f"{f}: {diff:.3e} of {scale:.3e}")
+    return bad
+
+
+@pytest.mark.parametrize("mesh", ["warped", "sedov15oct"])
+def test_matches_oracle(lulesh, oracle_mod, tmp_path, mesh):
+    """Against the CPU oracle's reading of the same file: a curvilinear,
+    renumbered -s 10 box (generated here), and the reference's own octant
+    mesh when its copy is present.  One cycle to rounding level, then the
+    full run to t = 0.01: same cycle count, origin energy within 1e-9."""
+    if mesh == "warped":
+        m = lmesh.box(10)
+        rng = np.random.default_rng(3)
+        path = str(tmp_path / "warped.lmesh")
+        lmesh.write(path, lmesh.renumber(lmesh.warp(m), rng.permutation(m.num_node),
+                                         rng.permutation(m.num_elem)))
+    else:
+        path = os.path.join(MESHES, "sedov15oct.lmesh")
+        if not os.path.exists(path):
+            pytest.skip("reference mesh copy absent")
+    m = lmesh.read(path)
+    E, N = m.num_elem, m.num_node
+    o = oracle_mod.Oracle.from_lmesh(path)
+    try:
+        with lulesh.LuleshSet.from_mesh(path, its=1) as s:
+            assert s.run() == lulesh.OK
+            assert o.step() == 0
+            bad = _compare(s, o, ELEM_FIELDS + NODE_FIELDS, E, N, 1e-12)
+            assert not bad, bad
+        o.close()
+        o = oracle_mod.Oracle.from_lmesh(path)
+        ost, ocyc = o.run()
+        with lulesh.LuleshSet.from_mesh(path) as s:
+            assert s.run() == ost == lulesh.OK
+            st = s.state()
+            assert st["cycle"] == ocyc
+            e_g, e_o = s.origin_energy(), o.origin_energy()
+            assert abs(e_g - e_o) <= 1e-9 * abs(e_o), (e_g, e_o)
+            bad = _compare(s, o, ["e", "p", "v", "x", "y", "z", "xd"], E, N, 1e-8)
+            assert not bad, bad
+    finally:
+        o.close()
+
+
 def test_reference_octant_mesh(lulesh):
     """The reference's own sedov15oct.lmesh (when its copy is present) runs
     to t = 0.01 with a finite, positive origin energy."""

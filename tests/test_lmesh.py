@@ -49,3 +49,35 @@ def test_renumber_keeps_geometry():
     # face neighbours map the same way
     assert (r.links[epm] == epm[m.links]).all()
     assert sorted(r.free) == sorted(npm[m.free])
+
+
+def test_oracle_reads_the_box_as_its_structured_mesh(oracle_mod, tmp_path):
+    """The oracle's lmesh reader (the -u branch of NewDomain) builds the same
+    tables from lmesh.box(nx) as its -s builder."""
+    p = tmp_path / "b6.lmesh"
+    lmesh.write(p, lmesh.box(6))
+    s, u = oracle_mod.Oracle(6), oracle_mod.Oracle.from_lmesh(str(p))
+    try:
+        for f in ["nodelist", "lxim", "lxip", "letam", "letap", "lzetam", "lzetap", "elemBC",
+                  "nodeElemStart", "nodeElemCornerList", "regElemlist", "regReps"]:
+            a, b = s.field(f), u.field(f)
+            n = min(len(a), len(b))
+            assert (a[:n] == b[:n]).all(), f
+        for f in ["x", "y", "z", "volo", "elemMass", "nodalMass"]:
+            assert (s.field(f) == u.field(f)).all(), f
+        # the deposit: 3.948746e7 at the octant corner (element 0 here)
+        assert u.field("e")[0] == 3.948746e7 and (u.field("e")[1:] == 0).all()
+    finally:
+        s.close()
+        u.close()
+
+
+def test_oracle_rejects_malformed_files(oracle_mod, tmp_path):
+    m = lmesh.box(2)
+    m.nodelist[1, 2] = 10 ** 6
+    p = tmp_path / "bad.lmesh"
+    lmesh.write(p, m)
+    with pytest.raises(ValueError):
+        oracle_mod.Oracle.from_lmesh(str(p))
+    with pytest.raises(ValueError):
+        oracle_mod.Oracle.from_lmesh(str(tmp_path / "absent.lmesh"))
