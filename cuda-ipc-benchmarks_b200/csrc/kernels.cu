@@ -259,7 +259,7 @@ __device__ __forceinline__ void advance_node(const DomDev &D, const TimeCtl &T, 
 // MODE 1: AddNodeForcesFromElems over this domain's own corners only,
 //         writing fx/fy/fz (the partial sums the reference exchanges).
 // MODE 2: the node update from fx/fy/fz (after CommSBN added neighbours).
-template <int MODE, int BS, bool U = false>
+template <int MODE, int BS>
 __global__ void __launch_bounds__(BS, min_blocks(kNodalMinBlocks, BS)) k_nodal(SetArgs a, Params P)
 {
     const int2 blk = a.blocks[blockIdx.x];
@@ -268,28 +268,14 @@ __global__ void __launch_bounds__(BS, min_blocks(kNodalMinBlocks, BS)) k_nodal(S
     if (!T.active) return;
     const int i = blk.y + threadIdx.x;
     if (i >= D.numNode) return;
-    int px = 0, py = 0, pz = 0;
-    if (!U) {
-        const int en = D.en;
-        px = i % en;
-        const int t = i / en;
-        py = t % en;
-        pz = t / en;
-    }
+    const int en = D.en;
+    const int px = i % en;
+    const int t = i / en;
+    const int py = t % en;
+    const int pz = t / en;
 
     double fx, fy, fz;
-    if (MODE == 0 && U) {
-        // AddNodeForcesFromElems (lulesh.cu:1715-1751): the node's corners
-        // in nodeElemCornerList order
-        fx = fy = fz = 0.0;
-        const int start = D.nodeElemStart[i], count = D.nodeElemCount[i];
-        for (int j = 0; j < count; ++j) {
-            const int k = D.nodeElemCornerList[start + j];
-            fx += ld_corner(D.fx_elem + k);
-            fy += ld_corner(D.fy_elem + k);
-            fz += ld_corner(D.fz_elem + k);
-        }
-    } else if (MODE == 0) {
+    if (MODE == 0) {
         gather_corners(a.doms, D, px, py, pz, fx, fy, fz);
     } else if (MODE == 1) {
         DomDev L = D;
@@ -306,21 +292,74 @@ __global__ void __launch_bounds__(BS, min_blocks(kNodalMinBlocks, BS)) k_nodal(S
     }
 
     // ApplyAccelerationBoundaryConditionsForNodes: symmetry planes are the
-    // px/py/pz == 0 node sets of the domains at the mesh origin faces (an
-    // unstructured mesh lists its symmetry nodes: nodeBC bits)
-    int bc;
-    if (U)
-        bc = D.nodeBC[i];
-    else
-        bc = (D.col == 0 && px == 0 ? 1 : 0) | (D.row == 0 && py == 0 ? 2 : 0) |
-             (D.plane == 0 && pz == 0 ? 4 : 0);
+    // px/py/pz == 0 node sets of the domains at the mesh origin faces
+    const int bc = (D.col == 0 && px == 0 ? 1 : 0) | (D.row == 0 && py == 0 ? 2 : 0) |
+                   (D.plane == 0 && pz == 0 ? 4 : 0);
     advance_node(D, T, P, i, bc, fx, fy, fz, a.materialize, MODE == 0);
+}
+
+// Unstructured meshes: AddNodeForcesFromElems (lulesh.cu:1715-1751) over
+// each node's run of nodeElemCornerList, in list order, then the node
+// update.  The runs of a block's consecutive nodes are contiguous in the
+// list; when they fit, the block stages them in shared memory with
+// coalesced loads (read straight from the list, each thread's run is an
+// 8-int stride: one sector per thread per load), and the corner loads go
+// out four corners at a time.
+template <int BS>
+__global__ void __launch_bounds__(BS, min_blocks(kNodalUMinBlocks, BS)) k_nodal_u(SetArgs a, Params P)
+{
+    __shared__ int s_list[8 * BS];
+    const int2 blk = a.blocks[blockIdx.x];
+    const DomDev &D = a.doms[blk.x];
+    const TimeCtl &T = a.tcs[D.tc];
+    if (!T.active) return;  // the whole block
+    const int first = blk.y;
+    const int last = min(first + BS, D.numNode) - 1;
+    const int lo = D.nodeElemStart[first];
+    const int len = D.nodeElemStart[last] + D.nodeElemCount[last] - lo;
+    const bool staged = len <= 8 * BS;
+    if (staged)
+        for (int k = threadIdx.x; k < len; k += BS) s_list[k] = D.nodeElemCornerList[lo + k];
+    __syncthreads();
+    const int i = first + threadIdx.x;
+    if (i > last) return;
+    const int start = D.nodeElemStart[i], count = D.nodeElemCount[i];
+    const int *list = staged ? s_list + (start - lo) : D.nodeElemCornerList + start;
+
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    int j = 0;
+    for (; j + 4 <= count; j += 4) {
+        int k[4];
+        double vx[4], vy[4], vz[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) k[q] = list[j + q];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            vx[q] = ld_corner(D.fx_elem + k[q]);
+            vy[q] = ld_corner(D.fy_elem + k[q]);
+            vz[q] = ld_corner(D.fz_elem + k[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            fx += vx[q];
+            fy += vy[q];
+            fz += vz[q];
+        }
+    }
+    for (; j < count; ++j) {
+        const int k = list[j];
+        fx += ld_corner(D.fx_elem + k);
+        fy += ld_corner(D.fy_elem + k);
+        fz += ld_corner(D.fz_elem + k);
+    }
+    // symmetry nodes of the mesh's X/Y/Z sets: nodeBC bits 0/1/2
+    advance_node(D, T, P, i, D.nodeBC[i], fx, fy, fz, a.materialize, true);
 }
 
 void launch_nodal(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs, bool u)
 {
     if (u) {
-        k_nodal<0, kNodeBlock, true><<<nblocks, kNodeBlock, 0, s>>>(a, P);
+        k_nodal_u<kNodeBlock><<<nblocks, kNodeBlock, 0, s>>>(a, P);
         return;
     }
     switch (bs) {

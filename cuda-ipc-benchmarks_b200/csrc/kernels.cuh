@@ -28,7 +28,12 @@ constexpr int kNodeBlock = 128;  // threads per block, node kernels
 #ifndef LULESH_NODAL_MINB
 #define LULESH_NODAL_MINB 16
 #endif
-constexpr int kNodalMinBlocks = LULESH_NODAL_MINB;constexpr int kForceMinBlocks = LULESH_FORCE_MINB;
+constexpr int kNodalMinBlocks = LULESH_NODAL_MINB;
+// unstructured nodal kernel: four corners x 3 components in flight
+#ifndef LULESH_NODAL_U_MINB
+#define LULESH_NODAL_U_MINB 12
+#endif
+constexpr int kNodalUMinBlocks = LULESH_NODAL_U_MINB;constexpr int kForceMinBlocks = LULESH_FORCE_MINB;
 constexpr int kKinMinBlocks = LULESH_KIN_MINB;
 constexpr int kEosMinBlocks = LULESH_EOS_MINB;
 

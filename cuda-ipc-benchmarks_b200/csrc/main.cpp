@@ -8,7 +8,9 @@
 //   omp form   -s -i -r -b -c -p -q -f -v -z -h (LULESH/omp_4.0/lulesh-util.cc:60-173)
 // plus -t TP (run as TP^3 in-device subdomains, the reference's TP^3-rank
 // run) and --staged (exchange halos through the CommSend/CommSBN/... message
-// sequence instead of the fused direct kernels), --mixed, --no-xyz.
+// sequence instead of the fused direct kernels), --mixed, --no-xyz,
+// --one-launch (the whole run as one graph launch with a device-side loop;
+// profilers cannot see into such a graph, so it is not the default).
 // Prints the report of VerifyAndWriteFinalOutput (lulesh.cu:4670-4750) with
 // the same lines and field positions, plus a full-precision energy line
 // and the true zone-cycles/s.
@@ -39,6 +41,7 @@ static void usage(const char *exe)
     std::printf(" --staged        : halo exchange through CommSend/CommSBN messages\n");
     std::printf(" --mixed         : FP32 element arithmetic, FP64 EOS/integration/dt\n");
     std::printf(" --no-xyz        : do not write xyz.asc\n");
+    std::printf(" --one-launch    : the whole run as one graph launch (device-side loop)\n");
     std::printf(" -h              : This message\n");
     std::printf(" -u <file.lmesh> : read an unstructured mesh instead of -s\n");
 }
@@ -65,6 +68,7 @@ int main(int argc, char *argv[])
     const double t_app_start = wall();
     int nx = 30, its = -1, nr = 11, balance = 1, cost = 1, tp = 1;
     bool quiet = false, progress = false, staged = false, mixed = false, xyz = true;
+    bool one_launch = false;
     std::string mesh;  // -u: an lmesh file
     // CUDA form: exactly "-s N x ITERS" or "-u FILE x ITERS" (argc == 5,
     // argv[4] the count)
@@ -112,6 +116,7 @@ int main(int argc, char *argv[])
             else if (a == "--staged") staged = true;
             else if (a == "--mixed") mixed = true;
             else if (a == "--no-xyz") xyz = false;
+            else if (a == "--one-launch") one_launch = true;
             else if (a == "-h") { usage(argv[0]); return 0; }
             else {
                 usage(argv[0]);
@@ -160,9 +165,12 @@ int main(int argc, char *argv[])
                     std::printf("cycle = %d, time = %e, dt=%e\n", s.cycle, s.time, s.deltatime);
                 st = lulesh_host_cycle(set.get(), nullptr, &s);
             }
-        } else {
+        } else if (one_launch) {
             // the whole run as one graph launch (device-side loop)
             st = lulesh_run_graph(set.get(), 0);
+        } else {
+            // one captured graph per cycle, the status read every 64 cycles
+            st = lulesh_run(set.get(), 64);
         }
         cudaDeviceSynchronize();
         const double elapsed = wall() - t0;

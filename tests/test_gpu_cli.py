@@ -80,3 +80,15 @@ def test_unstructured_form(tmp_path):
     full = [re.search(r"Origin energy, 17 digits = (\S+)", r.stdout).group(1) for r in (u, s)]
     assert full[0] == full[1]
     assert len(_awk(u.stdout, "FOM", 3)) == 1
+
+
+def test_one_launch_gives_the_same_run(tmp_path):
+    """--one-launch (the device-side loop) and the default per-cycle graph
+    launches print the same energy and iteration count."""
+    outs = [_run("-s", "12", "-i", "40", "--no-xyz", *extra, cwd=tmp_path)
+            for extra in ([], ["--one-launch"])]
+    for r in outs:
+        assert r.returncode == 0, r.stdout + r.stderr
+    full = [re.search(r"Origin energy, 17 digits = (\S+)", r.stdout).group(1) for r in outs]
+    assert full[0] == full[1]
+    assert _awk(outs[0].stdout, "Iteration count", 4) == _awk(outs[1].stdout, "Iteration count", 4)
