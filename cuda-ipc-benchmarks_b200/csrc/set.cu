@@ -242,9 +242,14 @@ int enqueue_cycle(lulesh_set *s)
 // cycle.  The access-policy window is a stream attribute, captured into
 // the cycle graph's kernel nodes.  Measured on B200 at -s 100: 339 -> 334
 // us per cycle.  Batches and subdomain sets do not use it.
+// 0 leaves every set's stream without an access-policy window
+#ifndef LULESH_L2_WINDOW
+#define LULESH_L2_WINDOW 1
+#endif
+
 static int l2_node_window(lulesh_set *s)
 {
-    if (s->ndom != 1) return LULESH_OK;
+    if (!LULESH_L2_WINDOW || s->ndom != 1) return LULESH_OK;
     const DomDev &D = s->hdoms[0];
     const char *lo = reinterpret_cast<const char *>(D.x);
     const char *hi = reinterpret_cast<const char *>(D.zd + D.numNode);
