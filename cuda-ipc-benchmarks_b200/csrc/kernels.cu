@@ -17,6 +17,9 @@
 //                   3988-4097, 4216-4403) fused; the dt minimum is reduced
 //                   with warp shuffles and one 64-bit atomicMin per block
 // Subdomain sets add two halo kernels (PosVel sync, MonoQ ghosts).
+// Unstructured (lmesh) domains run force, kinematics and EOS with U = true,
+// which reads nodelist, the face links and elemBC from memory instead of
+// computing them from the element index, and k_nodal_u for the nodal step.
 #include <climits>
 #include <cstdint>
 
