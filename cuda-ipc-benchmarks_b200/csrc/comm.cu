@@ -454,7 +454,7 @@ int comm_prepare(lulesh_set *s)
 int enqueue_cycle_staged(lulesh_set *s)
 {
     cudaStream_t st = s->stream;
-    launch_time_increment(s->dtc, s->njobs, s->P, st);
+    launch_time_increment(s->dtc, s->njobs, s->P, st, s->pdl);
     launch_force_fp64(s, st);
     // AddNodeForcesFromElems over local corners only, then SBN exchange
     launch_nodal_gather_local(s->args(s->node_blocks), s->n_node_blocks, st);

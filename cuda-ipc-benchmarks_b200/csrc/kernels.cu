@@ -30,6 +30,39 @@
 namespace lulesh {
 
 // ---------------------------------------------------------------------------
+// programmatic dependent launch
+//
+// The cycle kernels may be launched with programmatic stream serialisation
+// (SetArgs::pdl): the next kernel's blocks are then scheduled while this
+// one's last wave drains.  Every such kernel starts with pdl_enter(): it
+// waits until the previous grid has completed and its writes are visible,
+// before touching any memory, then lets its own dependents be scheduled.
+// A kernel launched without the attribute passes through both at once.
+
+__device__ __forceinline__ void pdl_enter()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+static void launch_k(void (*kernel)(KArgs...), int grid, int block, cudaStream_t s, bool pdl,
+                     Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = pdl ? attr : nullptr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
+// ---------------------------------------------------------------------------
 // time increment
 
 __device__ __forceinline__ unsigned long long dbits(double v)
@@ -39,6 +72,7 @@ __device__ __forceinline__ unsigned long long dbits(double v)
 
 __global__ void k_time_increment(TimeCtl *tcs, int ntc, Params P)
 {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ntc) return;
     TimeCtl &T = tcs[i];
@@ -97,10 +131,10 @@ __global__ void k_time_increment(TimeCtl *tcs, int ntc, Params P)
     T.active = 1;
 }
 
-void launch_time_increment(TimeCtl *tcs, int ntc, Params P, cudaStream_t s)
+void launch_time_increment(TimeCtl *tcs, int ntc, Params P, cudaStream_t s, bool pdl)
 {
     const int b = 128;
-    k_time_increment<<<(ntc + b - 1) / b, b, 0, s>>>(tcs, ntc, P);
+    launch_k(k_time_increment, (ntc + b - 1) / b, b, s, pdl, tcs, ntc, P);
 }
 
 // ---------------------------------------------------------------------------
@@ -118,6 +152,7 @@ __device__ __constant__ int kCZ[8] = {0, 0, 0, 0, 1, 1, 1, 1};
 template <bool HG, int BS, bool U>
 __global__ void __launch_bounds__(BS, min_blocks(kForceMinBlocks, BS)) k_force(SetArgs a, Params P)
 {
+    pdl_enter();
     const int2 blk = a.blocks[blockIdx.x];
     const DomDev &D = a.doms[blk.x];
     TimeCtl &T = a.tcs[D.tc];
@@ -156,9 +191,9 @@ template <int BS, bool U = false>
 static void launch_force_bs(const SetArgs &a, int nblocks, Params P, cudaStream_t s)
 {
     if (P.hgcoef > 0.0)
-        k_force<true, BS, U><<<nblocks, BS, 0, s>>>(a, P);
+        launch_k(k_force<true, BS, U>, nblocks, BS, s, a.pdl != 0, a, P);
     else
-        k_force<false, BS, U><<<nblocks, BS, 0, s>>>(a, P);
+        launch_k(k_force<false, BS, U>, nblocks, BS, s, a.pdl != 0, a, P);
 }
 
 void launch_force(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs, bool u)
@@ -265,6 +300,7 @@ __device__ __forceinline__ void advance_node(const DomDev &D, const TimeCtl &T, 
 template <int MODE, int BS>
 __global__ void __launch_bounds__(BS, min_blocks(kNodalMinBlocks, BS)) k_nodal(SetArgs a, Params P)
 {
+    pdl_enter();
     const int2 blk = a.blocks[blockIdx.x];
     const DomDev &D = a.doms[blk.x];
     const TimeCtl &T = a.tcs[D.tc];
@@ -311,6 +347,7 @@ __global__ void __launch_bounds__(BS, min_blocks(kNodalMinBlocks, BS)) k_nodal(S
 template <int BS>
 __global__ void __launch_bounds__(BS, min_blocks(kNodalUMinBlocks, BS)) k_nodal_u(SetArgs a, Params P)
 {
+    pdl_enter();
     __shared__ int s_list[8 * BS];
     const int2 blk = a.blocks[blockIdx.x];
     const DomDev &D = a.doms[blk.x];
@@ -362,13 +399,13 @@ __global__ void __launch_bounds__(BS, min_blocks(kNodalUMinBlocks, BS)) k_nodal_
 void launch_nodal(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs, bool u)
 {
     if (u) {
-        k_nodal_u<kNodeBlock><<<nblocks, kNodeBlock, 0, s>>>(a, P);
+        launch_k(k_nodal_u<kNodeBlock>, nblocks, kNodeBlock, s, a.pdl != 0, a, P);
         return;
     }
     switch (bs) {
-        case 256: k_nodal<0, 256><<<nblocks, 256, 0, s>>>(a, P); break;
-        case 512: k_nodal<0, 512><<<nblocks, 512, 0, s>>>(a, P); break;
-        default: k_nodal<0, kNodeBlock><<<nblocks, kNodeBlock, 0, s>>>(a, P); break;
+        case 256: launch_k(k_nodal<0, 256>, nblocks, 256, s, a.pdl != 0, a, P); break;
+        case 512: launch_k(k_nodal<0, 512>, nblocks, 512, s, a.pdl != 0, a, P); break;
+        default: launch_k(k_nodal<0, kNodeBlock>, nblocks, kNodeBlock, s, a.pdl != 0, a, P); break;
     }
 }
 
@@ -388,6 +425,7 @@ void launch_nodal_update(const SetArgs &a, int nblocks, Params P, cudaStream_t s
 template <int BS, bool U = false>
 __global__ void __launch_bounds__(BS, min_blocks(kKinMinBlocks, BS)) k_kinematics(SetArgs a)
 {
+    pdl_enter();
     const int2 blk = a.blocks[blockIdx.x];
     const DomDev &D = a.doms[blk.x];
     TimeCtl &T = a.tcs[D.tc];
@@ -420,13 +458,13 @@ void launch_kinematics(const SetArgs &a, int nblocks, Params P, cudaStream_t s, 
 {
     (void)P;
     if (u) {
-        k_kinematics<kElemBlock, true><<<nblocks, kElemBlock, 0, s>>>(a);
+        launch_k(k_kinematics<kElemBlock, true>, nblocks, kElemBlock, s, a.pdl != 0, a);
         return;
     }
     switch (bs) {
-        case 64: k_kinematics<64><<<nblocks, 64, 0, s>>>(a); break;
-        case 256: k_kinematics<256><<<nblocks, 256, 0, s>>>(a); break;
-        default: k_kinematics<kElemBlock><<<nblocks, kElemBlock, 0, s>>>(a); break;
+        case 64: launch_k(k_kinematics<64>, nblocks, 64, s, a.pdl != 0, a); break;
+        case 256: launch_k(k_kinematics<256>, nblocks, 256, s, a.pdl != 0, a); break;
+        default: launch_k(k_kinematics<kElemBlock>, nblocks, kElemBlock, s, a.pdl != 0, a); break;
     }
 }
 
@@ -598,6 +636,7 @@ __device__ __forceinline__ double warp_min(double v)
 template <int BS, bool U = false>
 __global__ void __launch_bounds__(BS, min_blocks(kEosMinBlocks, BS)) k_eos(SetArgs a, Params P)
 {
+    pdl_enter();
     const int2 blk = a.blocks[blockIdx.x];
     const DomDev &D = a.doms[blk.x];
     TimeCtl &T = a.tcs[D.tc];
@@ -780,13 +819,13 @@ __global__ void __launch_bounds__(BS, min_blocks(kEosMinBlocks, BS)) k_eos(SetAr
 void launch_eos(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs, bool u)
 {
     if (u) {
-        k_eos<kElemBlock, true><<<nblocks, kElemBlock, 0, s>>>(a, P);
+        launch_k(k_eos<kElemBlock, true>, nblocks, kElemBlock, s, a.pdl != 0, a, P);
         return;
     }
     switch (bs) {
-        case 64: k_eos<64><<<nblocks, 64, 0, s>>>(a, P); break;
-        case 256: k_eos<256><<<nblocks, 256, 0, s>>>(a, P); break;
-        default: k_eos<kElemBlock><<<nblocks, kElemBlock, 0, s>>>(a, P); break;
+        case 64: launch_k(k_eos<64>, nblocks, 64, s, a.pdl != 0, a, P); break;
+        case 256: launch_k(k_eos<256>, nblocks, 256, s, a.pdl != 0, a, P); break;
+        default: launch_k(k_eos<kElemBlock>, nblocks, kElemBlock, s, a.pdl != 0, a, P); break;
     }
 }
 

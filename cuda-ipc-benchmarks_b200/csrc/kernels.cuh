@@ -56,9 +56,12 @@ struct SetArgs {
     TimeCtl *tcs;
     const int2 *blocks;
     int materialize;  // also write the per-cycle transients
+    // launch with programmatic stream serialisation (host side only; the
+    // kernels launched this way wait for the previous grid first)
+    int pdl = 0;
 };
 
-void launch_time_increment(TimeCtl *tcs, int ntc, Params P, cudaStream_t s);
+void launch_time_increment(TimeCtl *tcs, int ntc, Params P, cudaStream_t s, bool pdl = false);
 // u: the set's domains are unstructured (lmesh): 128-wide blocks, mesh
 // arrays read instead of structured indexing
 void launch_force(const SetArgs &a, int nblocks, Params P, cudaStream_t s,

@@ -63,7 +63,11 @@ int ensure_run_graph(lulesh_set *s)
                                                        cudaStreamCaptureModeThreadLocal),
                          "capture loop body");
         if (st == LULESH_OK) {
+            // the loop body keeps plain stream order between its kernels
+            const bool pdl = s->pdl;
+            s->pdl = false;
             int est = enqueue_cycle(s);
+            s->pdl = pdl;
             k_run_continue<<<1, 128, 0, s->stream>>>(h, s->dtc, s->njobs, s->run_ctl);
             cudaGraph_t captured = nullptr;
             const int cst = cuda_status(cudaStreamEndCapture(s->stream, &captured), "end capture");

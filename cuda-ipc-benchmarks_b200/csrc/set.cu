@@ -214,7 +214,7 @@ int enqueue_cycle(lulesh_set *s)
     if (s->flags & LULESH_FLAG_COMM_STAGED) return enqueue_cycle_staged(s);
     cudaStream_t st = s->stream;
     const bool mixed = (s->flags & LULESH_FLAG_MIXED) != 0;
-    launch_time_increment(s->dtc, s->njobs, s->P, st);
+    launch_time_increment(s->dtc, s->njobs, s->P, st, s->pdl);
     if (mixed)
         launch_force_mixed(s->args(s->elem_blocks), s->n_elem_blocks, s->P, s->dcorner32, st);
     else
@@ -743,7 +743,7 @@ int lulesh_profile_phases(lulesh_set *s, int ncycles, double *ms_out, int *nphas
     const bool mixed = (s->flags & LULESH_FLAG_MIXED) != 0;
     for (int c = 0; c < ncycles; ++c) {
         LCHECK(cudaEventRecord(ev[0], st));
-        launch_time_increment(s->dtc, s->njobs, s->P, st);
+        launch_time_increment(s->dtc, s->njobs, s->P, st, s->pdl);
         LCHECK(cudaEventRecord(ev[1], st));
         if (mixed)
             launch_force_mixed(s->args(s->elem_blocks), s->n_elem_blocks, s->P, s->dcorner32, st);

@@ -11,6 +11,11 @@
 #include "lulesh_b200.h"
 #include "lulesh_dev.h"
 
+// 0 launches every cycle kernel with plain stream order
+#ifndef LULESH_PDL
+#define LULESH_PDL 1
+#endif
+
 struct lulesh_set {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -48,6 +53,8 @@ struct lulesh_set {
 
     // L2 access-policy window set on `stream` (single domains)
     bool l2_window = false;
+    // launch the cycle kernels with programmatic dependent launch
+    bool pdl = LULESH_PDL != 0;
 
     // the arena
     void *arena = nullptr;
@@ -79,6 +86,7 @@ struct lulesh_set {
         a.tcs = dtc;
         a.blocks = blocks;
         a.materialize = (flags & LULESH_FLAG_MATERIALIZE) ? 1 : 0;
+        a.pdl = pdl ? 1 : 0;
         return a;
     }
 };
