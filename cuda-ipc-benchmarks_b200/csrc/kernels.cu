@@ -30,39 +30,6 @@
 namespace lulesh {
 
 // ---------------------------------------------------------------------------
-// programmatic dependent launch
-//
-// The cycle kernels may be launched with programmatic stream serialisation
-// (SetArgs::pdl): the next kernel's blocks are then scheduled while this
-// one's last wave drains.  Every such kernel starts with pdl_enter(): it
-// waits until the previous grid has completed and its writes are visible,
-// before touching any memory, then lets its own dependents be scheduled.
-// A kernel launched without the attribute passes through both at once.
-
-__device__ __forceinline__ void pdl_enter()
-{
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
-
-template <typename... KArgs, typename... Args>
-static void launch_k(void (*kernel)(KArgs...), int grid, int block, cudaStream_t s, bool pdl,
-                     Args... args)
-{
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)grid);
-    cfg.blockDim = dim3((unsigned)block);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = pdl ? attr : nullptr;
-    cfg.numAttrs = pdl ? 1 : 0;
-    cudaLaunchKernelEx(&cfg, kernel, args...);
-}
-
-// ---------------------------------------------------------------------------
 // time increment
 
 __device__ __forceinline__ unsigned long long dbits(double v)

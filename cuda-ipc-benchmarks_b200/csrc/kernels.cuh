@@ -61,6 +61,39 @@ struct SetArgs {
     int pdl = 0;
 };
 
+// ---------------------------------------------------------------------------
+// programmatic dependent launch
+//
+// The cycle kernels may be launched with programmatic stream serialisation
+// (SetArgs::pdl): the next kernel's blocks are then scheduled while this
+// one's last wave drains.  Every kernel launched that way starts with
+// pdl_enter(): it waits until the previous grid has completed and its
+// writes are visible, before touching any memory, then lets its own
+// dependents be scheduled.  Without the attribute both pass at once.
+
+__device__ __forceinline__ void pdl_enter()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+inline void launch_k(void (*kernel)(KArgs...), int grid, int block, cudaStream_t s, bool pdl,
+                     Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = pdl ? attr : nullptr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kernel, args...);  // errors: cudaGetLastError
+}
+
 void launch_time_increment(TimeCtl *tcs, int ntc, Params P, cudaStream_t s, bool pdl = false);
 // u: the set's domains are unstructured (lmesh): 128-wide blocks, mesh
 // arrays read instead of structured indexing

@@ -50,6 +50,7 @@ template <bool HG>
 __global__ void __launch_bounds__(kElemBlock, LULESH_MIXED_FORCE_MINB)
     k_force_mixed(SetArgs a, Params P, const CornerF32 *cfs)
 {
+    pdl_enter();
     const int2 blk = a.blocks[blockIdx.x];
     const DomDev &D = a.doms[blk.x];
     TimeCtl &T = a.tcs[D.tc];
@@ -121,9 +122,9 @@ void launch_force_mixed(const SetArgs &a, int nblocks, Params P, const CornerF32
                         cudaStream_t s)
 {
     if (P.hgcoef > 0.0)
-        k_force_mixed<true><<<nblocks, kElemBlock, 0, s>>>(a, P, cf);
+        launch_k(k_force_mixed<true>, nblocks, kElemBlock, s, a.pdl != 0, a, P, cf);
     else
-        k_force_mixed<false><<<nblocks, kElemBlock, 0, s>>>(a, P, cf);
+        launch_k(k_force_mixed<false>, nblocks, kElemBlock, s, a.pdl != 0, a, P, cf);
 }
 
 // Neumaier's compensated addition: s + c carries the sum of all terms
@@ -140,6 +141,7 @@ __device__ __forceinline__ void comp_add(float &s, float &c, float v)
 __global__ void __launch_bounds__(kNodeBlock, min_blocks(kNodalMinBlocks, kNodeBlock))
     k_nodal_mixed(SetArgs a, Params P, const CornerF32 *cfs)
 {
+    pdl_enter();
     const int2 blk = a.blocks[blockIdx.x];
     const DomDev &D = a.doms[blk.x];
     const TimeCtl &T = a.tcs[D.tc];
@@ -197,12 +199,13 @@ __global__ void __launch_bounds__(kNodeBlock, min_blocks(kNodalMinBlocks, kNodeB
 void launch_nodal_mixed(const SetArgs &a, int nblocks, Params P, const CornerF32 *cf,
                         cudaStream_t s)
 {
-    k_nodal_mixed<<<nblocks, kNodeBlock, 0, s>>>(a, P, cf);
+    launch_k(k_nodal_mixed, nblocks, kNodeBlock, s, a.pdl != 0, a, P, cf);
 }
 
 __global__ void __launch_bounds__(kElemBlock, LULESH_MIXED_KIN_MINB)
     k_kinematics_mixed(SetArgs a, Params P)
 {
+    pdl_enter();
     const int2 blk = a.blocks[blockIdx.x];
     const DomDev &D = a.doms[blk.x];
     TimeCtl &T = a.tcs[D.tc];
@@ -266,7 +269,7 @@ __global__ void __launch_bounds__(kElemBlock, LULESH_MIXED_KIN_MINB)
 
 void launch_kinematics_mixed(const SetArgs &a, int nblocks, Params P, cudaStream_t s)
 {
-    k_kinematics_mixed<<<nblocks, kElemBlock, 0, s>>>(a, P);
+    launch_k(k_kinematics_mixed, nblocks, kElemBlock, s, a.pdl != 0, a, P);
 }
 
 }  // namespace lulesh
