@@ -33,7 +33,8 @@ constexpr int kNodalMinBlocks = LULESH_NODAL_MINB;
 #ifndef LULESH_NODAL_U_MINB
 #define LULESH_NODAL_U_MINB 12
 #endif
-constexpr int kNodalUMinBlocks = LULESH_NODAL_U_MINB;constexpr int kForceMinBlocks = LULESH_FORCE_MINB;
+constexpr int kNodalUMinBlocks = LULESH_NODAL_U_MINB;
+constexpr int kForceMinBlocks = LULESH_FORCE_MINB;
 constexpr int kKinMinBlocks = LULESH_KIN_MINB;
 constexpr int kEosMinBlocks = LULESH_EOS_MINB;
 
