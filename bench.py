@@ -1,6 +1,6 @@
 """Benchmark: LULESH sedov Lagrange step, zone-cycles/s on B200.
 
-Workload (BASELINE metric "zone-cycles/s at -s 100 on 1 B200"): one domain of
+Workload (the headline metric, zone-cycles/s at -s 100 on one B200): one domain of
 -s 100 (1,000,000 hex elements, 1,030,301 nodes), FP64, 11 regions, balance 1,
 cost 1.  A step is one cycle (TimeIncrement + LagrangeLeapFrog) over the
 whole mesh.  State (~0.57 GB) is far larger than the 126 MB L2, so no flush
@@ -35,6 +35,7 @@ import json
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -108,7 +109,8 @@ class ClockSampler:
         self.path = None
 
     def start(self):
-        out_dir = os.path.join(REPO, "gpurun_out")
+        # the samples go to BENCH_CLOCKS_DIR (default: the system temp dir)
+        out_dir = os.environ.get("BENCH_CLOCKS_DIR") or tempfile.gettempdir()
         os.makedirs(out_dir, exist_ok=True)
         self.path = os.path.join(out_dir, f"clocks_gpu{self.gpu}_{os.getpid()}.csv")
         try:

@@ -3,7 +3,7 @@
 Tolerances.  The oracle evaluates the reference's expressions without FMA
 contraction; the GPU build contracts multiply-adds like the reference CUDA
 build does.  Fields therefore agree to rounding level after one cycle
-(rtol 1e-12) and drift slowly; the north-star gate is Final Origin Energy
+(rtol 1e-12) and drift slowly; the parity gate is Final Origin Energy
 within 1e-9 relative.
 """
 import json
@@ -16,7 +16,7 @@ from conftest import GOLDEN, rel
 
 pytestmark = pytest.mark.gpu
 
-E_TOL = 1e-9  # Final Origin Energy, relative
+E_TOL = 1e-9  # Final Origin Energy, relative (the parity bound)
 
 ELEM_FIELDS = ["e", "p", "q", "v", "ss", "delv", "vdov", "arealg", "ql", "qq", "vnew",
                "delx_xi", "delx_eta", "delx_zeta"]
