@@ -51,10 +51,15 @@ ZONES = NX ** 3
 METRIC = "zone-cycles/s at -s 100 on 1 B200"
 UNIT = "zone-cycles/s"
 # Algorithmic bytes per zone-cycle of each phase (compulsory traffic at the
-# four dependency boundaries of the step, FP64): force 152, nodal update 128,
-# kinematics + monoQ gradient 176, monoQ region + EOS + volume + dt 204.
-ALG_BYTES = {"force": 152.0, "nodal": 128.0, "kinematics": 176.0, "eos": 204.0}
-ALG_BYTES_STEP = 660.0
+# four dependency boundaries of the step, enumerated array by array in
+# bytes_model.py): force 152, nodal update 128, kinematics + monoQ gradient
+# 176, monoQ region + EOS + volume + dt 196; 652 per cycle.  This build's own
+# traffic (corner forces written and read back) is 896.
+import bytes_model  # noqa: E402
+
+ALG_BYTES = {k: float(v) for k, v in bytes_model.phase_bytes().items()}
+ALG_BYTES_STEP = bytes_model.step_bytes()
+BUILD_BYTES_STEP = bytes_model.step_bytes(bytes_model.THIS_BUILD)
 LAUNCHES_PER_CYCLE = 5  # time_increment, force, nodal, kinematics, eos
 # FP64 flops per element of each phase (an FMA counts 2), measured with
 # ncu's smsp__sass_thread_inst_executed_op_{dfma,dadd,dmul}_pred_on counters
@@ -278,6 +283,7 @@ def run_ours(a, rank, world, local_rank):
     fp64_peak = fp64_peak_tflops(dev)
     fp64 = {k: FP64_FLOPS[k] * ZONES / (phases[k] / 1e3) / 1e12 for k in FP64_FLOPS}
     ach_step = ALG_BYTES_STEP * ZONES / (ms / a.steps / 1e3) / 1e9
+    ach_build = BUILD_BYTES_STEP * ZONES / (ms / a.steps / 1e3) / 1e9
 
     # end-to-end through the host-driven C-ABI call
     e2e_n = min(a.steps, a.e2e_cycles)
@@ -343,7 +349,9 @@ def run_ours(a, rank, world, local_rank):
                                       for k, v in fp64.items()},
                           "flops_per_element": FP64_FLOPS},
         "roofline_step": {"achieved": ach_step, "frac": ach_step / peak,
-                          "alg_bytes_per_zone_cycle": ALG_BYTES_STEP},
+                          "alg_bytes_per_zone_cycle": ALG_BYTES_STEP,
+                          "build_bytes_per_zone_cycle": BUILD_BYTES_STEP,
+                          "build_achieved": ach_build, "build_frac": ach_build / peak},
         "phases_ms": phases, "phases_sum_ms": step_ms_sum,
         "clocks": ck, "origin_energy": energy, "cycles_run": total,
         "cpu_baseline": cpu,
