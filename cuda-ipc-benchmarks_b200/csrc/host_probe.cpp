@@ -15,15 +15,10 @@ void lulesh_host_rand(unsigned seed, int n, int *out)
     for (int i = 0; i < n; ++i) out[i] = r.next();
 }
 
-// Build one domain and copy the named array into out (capacity `cap`
-// elements of the array's type); returns the array length, -1 if unknown.
-long lulesh_host_domain_field(int nx, int tp, int col, int row, int plane, int rank,
-                              int numReg, int balance, int cost, int global_mass,
-                              const char *name, void *out, long cap)
+// Copy the named array of a built domain into out (capacity `cap` elements
+// of the array's type); returns the array length, -1 if unknown.
+static long copy_field(const lulesh::HostDomain &d, const char *name, void *out, long cap)
 {
-    lulesh::HostDomain d;
-    lulesh::build_domain(d, nx, tp, col, row, plane, rank, numReg, balance, cost,
-                         global_mass != 0);
     struct I {
         const char *n;
         const std::vector<int> *v;
@@ -35,7 +30,8 @@ long lulesh_host_domain_field(int nx, int tp, int col, int row, int plane, int r
                 {"symmY", &d.symmY}, {"symmZ", &d.symmZ}, {"matElemlist", &d.matElemlist},
                 {"regElemSize", &d.regElemSize}, {"regCSR", &d.regCSR},
                 {"regReps", &d.regReps}, {"regNumList", &d.regNumList},
-                {"regElemlist", &d.regElemlist}, {"regSorted", &d.regSorted}};
+                {"regElemlist", &d.regElemlist}, {"regSorted", &d.regSorted},
+                {"nodeBC", &d.nodeBC}};
     struct R {
         const char *n;
         const std::vector<double> *v;
@@ -57,7 +53,32 @@ long lulesh_host_domain_field(int nx, int tp, int col, int row, int plane, int r
         if (out && cap >= 1) *(double *)out = d.deltatime;
         return 1;
     }
+    if (!std::strcmp(name, "octant")) {
+        if (out && cap >= 1) *(int *)out = d.octantCorner;
+        return 1;
+    }
     return -1;
+}
+
+// Build one structured domain and copy the named array (copy_field).
+long lulesh_host_domain_field(int nx, int tp, int col, int row, int plane, int rank,
+                              int numReg, int balance, int cost, int global_mass,
+                              const char *name, void *out, long cap)
+{
+    lulesh::HostDomain d;
+    lulesh::build_domain(d, nx, tp, col, row, plane, rank, numReg, balance, cost,
+                         global_mass != 0);
+    return copy_field(d, name, out, cap);
+}
+
+// Read one domain from an lmesh file (lulesh_create_from_mesh's reader) and
+// copy the named array; -2 if the file is unreadable or malformed.
+long lulesh_host_lmesh_field(const char *path, int numReg, int balance, int cost,
+                             const char *name, void *out, long cap)
+{
+    lulesh::HostDomain d;
+    if (!lulesh::build_domain_lmesh(d, path, numReg, balance, cost, nullptr)) return -2;
+    return copy_field(d, name, out, cap);
 }
 
 }  // extern "C"

@@ -1,6 +1,8 @@
 """The lmesh writer/reader (the reference's -u input format, lulesh.cu:855-1052):
 the cube it writes is the -s mesh of the oracle's BuildMesh restatement, and
 files round-trip exactly."""
+import os
+
 import numpy as np
 import pytest
 
@@ -81,3 +83,79 @@ def test_oracle_rejects_malformed_files(oracle_mod, tmp_path):
         oracle_mod.Oracle.from_lmesh(str(p))
     with pytest.raises(ValueError):
         oracle_mod.Oracle.from_lmesh(str(tmp_path / "absent.lmesh"))
+
+
+LMESH_FIELDS = ["nodelist", "lxim", "lxip", "letam", "letap", "lzetam", "lzetap", "elemBC",
+                "nodeElemCount", "nodeElemStart", "nodeElemCornerList", "symmX", "symmY",
+                "symmZ", "matElemlist", "regElemSize", "regCSR", "regReps", "regNumList",
+                "regElemlist", "regSorted", "x", "y", "z", "volo", "elemMass", "nodalMass",
+                "e"]
+
+
+def _host_lmesh(path, name):
+    import ctypes
+
+    from conftest import PKG
+    from oracle import INT_FIELDS
+
+    lib = ctypes.CDLL(os.path.join(PKG, "liblulesh_host.so"))
+    f = lib.lulesh_host_lmesh_field
+    f.restype = ctypes.c_long
+    f.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p,
+                  ctypes.c_void_p, ctypes.c_long]
+    n = f(str(path).encode(), 11, 1, 1, name.encode(), None, 0)
+    assert n >= 0, (name, n)
+    dt = np.int32 if name in INT_FIELDS or name == "octant" else np.float64
+    out = np.empty(n, dtype=dt)
+    f(str(path).encode(), 11, 1, 1, name.encode(), out.ctypes.data_as(ctypes.c_void_p), n)
+    return out
+
+
+def _meshes(tmp_path):
+    m = lmesh.box(9)
+    rng = np.random.default_rng(5)
+    p = tmp_path / "warped.lmesh"
+    lmesh.write(p, lmesh.renumber(lmesh.warp(m), rng.permutation(m.num_node),
+                                  rng.permutation(m.num_elem)))
+    out = [p]
+    ref = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle",
+                       "_ref", "meshes", "sedov15oct.lmesh")
+    if os.path.exists(ref):
+        out.append(ref)
+    return out
+
+
+def test_product_reader_matches_the_oracle(oracle_mod, tmp_path):
+    """The product's lmesh reader (lulesh_create_from_mesh, C++) and the
+    oracle's (C) build the same domain bit for bit: connectivity, boundary
+    masks with the *_FREE free surface, corner lists, regions, geometry,
+    masses, the octant-corner deposit and the initial dt."""
+    for path in _meshes(tmp_path):
+        o = oracle_mod.Oracle.from_lmesh(str(path))
+        try:
+            for f in LMESH_FIELDS:
+                a, b = _host_lmesh(path, f), o.field(f)
+                assert a.shape == b.shape and np.array_equal(a, b), (path, f)
+            assert _host_lmesh(path, "deltatime")[0] == o.scalar("deltatime")
+            oct_ = int(_host_lmesh(path, "octant")[0])
+            assert o.field("e")[oct_] == 3.948746e7
+        finally:
+            o.close()
+
+
+def test_product_reader_rejects_malformed_files(tmp_path):
+    import ctypes
+
+    from conftest import PKG
+
+    lib = ctypes.CDLL(os.path.join(PKG, "liblulesh_host.so"))
+    f = lib.lulesh_host_lmesh_field
+    f.restype = ctypes.c_long
+    f.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p,
+                  ctypes.c_void_p, ctypes.c_long]
+    m = lmesh.box(2)
+    m.links[3, 4] = m.num_elem
+    p = tmp_path / "bad.lmesh"
+    lmesh.write(p, m)
+    assert f(str(p).encode(), 11, 1, 1, b"x", None, 0) == -2
+    assert f(str(tmp_path / "none.lmesh").encode(), 11, 1, 1, b"x", None, 0) == -2
