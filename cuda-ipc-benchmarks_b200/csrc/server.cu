@@ -107,7 +107,7 @@ struct lulesh_server {
         a.tcs = dtc;
         a.blocks = b;
         a.materialize = 0;
-        a.pdl = 1;  // the cycle kernels overlap each other's tails
+        a.pdl = LULESH_PDL;  // the cycle kernels overlap each other's tails
         return a;
     }
 };
@@ -191,7 +191,7 @@ static int rebuild(lulesh_server *s)
         s->graph = nullptr;
     } else {
         SCHECK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-        launch_time_increment(s->dtc, s->cfg.max_jobs, s->P, s->stream, true);
+        launch_time_increment(s->dtc, s->cfg.max_jobs, s->P, s->stream, LULESH_PDL != 0);
         launch_force(s->args(s->elem_b), s->n_elem, s->P, s->stream);
         launch_nodal(s->args(s->node_b), s->n_node, s->P, s->stream);
         launch_kinematics(s->args(s->elem_b), s->n_elem, s->P, s->stream);
