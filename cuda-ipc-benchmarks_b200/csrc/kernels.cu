@@ -35,6 +35,9 @@
 #ifndef LULESH_KIN_REVERSE
 #define LULESH_KIN_REVERSE 1
 #endif
+#ifndef LULESH_FORCE_REVERSE
+#define LULESH_FORCE_REVERSE 0
+#endif
 #ifndef LULESH_EOS_REVERSE
 #define LULESH_EOS_REVERSE 0
 #endif
@@ -132,7 +135,7 @@ template <bool HG, int BS, bool U>
 __global__ void __launch_bounds__(BS, min_blocks(kForceMinBlocks, BS)) k_force(SetArgs a, Params P)
 {
     pdl_enter();
-    const int2 blk = a.blocks[blockIdx.x];
+    const int2 blk = a.blocks[LULESH_FORCE_REVERSE ? gridDim.x - 1 - blockIdx.x : blockIdx.x];
     const DomDev &D = a.doms[blk.x];
     TimeCtl &T = a.tcs[D.tc];
     if (!T.active) return;
