@@ -27,21 +27,6 @@
 #include "elem_math.cuh"
 #include "kernels.cuh"
 
-// Block order of the kinematics and EOS launches.  Kinematics walks its
-// block table last to first: its last outputs are then those of the first
-// elements, where each rep class of the EOS walk starts, and they are still
-// in L2 (measured on B200 at -s 100: EOS 91 -> 86 us, cycle 329 -> 325 us,
-// the same results).  Reversing the EOS walk instead gained nothing.
-#ifndef LULESH_KIN_REVERSE
-#define LULESH_KIN_REVERSE 1
-#endif
-#ifndef LULESH_FORCE_REVERSE
-#define LULESH_FORCE_REVERSE 0
-#endif
-#ifndef LULESH_EOS_REVERSE
-#define LULESH_EOS_REVERSE 0
-#endif
-
 namespace lulesh {
 
 // ---------------------------------------------------------------------------

@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(kElemBlock, LULESH_MIXED_KIN_MINB)
     k_kinematics_mixed(SetArgs a, Params P)
 {
     pdl_enter();
-    const int2 blk = a.blocks[blockIdx.x];
+    const int2 blk = a.blocks[LULESH_KIN_REVERSE ? gridDim.x - 1 - blockIdx.x : blockIdx.x];
     const DomDev &D = a.doms[blk.x];
     TimeCtl &T = a.tcs[D.tc];
     if (!T.active) return;

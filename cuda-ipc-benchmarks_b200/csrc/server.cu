@@ -152,6 +152,8 @@ static int rebuild(lulesh_server *s)
         for (int i = 0; i < D.numNode; i += kNodeBlock) nb.push_back(make_int2((int)d, i));
         for (int i = 0; i < D.numElem; i += kElemBlock) eb.push_back(make_int2((int)d, i));
     }
+    // the nodal kernel walks last to first, as for sets (build_tables)
+    if (LULESH_NODAL_REVERSE) std::reverse(nb.begin(), nb.end());
     if (!hd.empty())
         SCHECK(cudaMemcpyAsync(s->ddoms, hd.data(), sizeof(DomDev) * hd.size(),
                                cudaMemcpyHostToDevice, s->stream));

@@ -71,12 +71,7 @@ int build_tables(lulesh_set *s)
                     for (int i = 0; i < D.nx * D.nx; i += kElemBlock)
                         gb.push_back(make_int2(d, (f << 24) | i));
     }
-    // node blocks last-to-first: the nodal kernel follows the force kernel,
-    // whose last-written corner forces are the ones still in L2 (measured on
-    // B200 at -s 100: nodal 53.7 -> 48.9 us, the same results)
-#ifndef LULESH_NODAL_REVERSE
-#define LULESH_NODAL_REVERSE 1
-#endif
+    // node blocks last-to-first (LULESH_NODAL_REVERSE, set.hpp)
     if (LULESH_NODAL_REVERSE) std::reverse(nb.begin(), nb.end());
     s->n_elem_blocks = (int)eb.size();
     s->n_node_blocks = (int)nb.size();
