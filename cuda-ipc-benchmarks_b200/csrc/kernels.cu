@@ -26,6 +26,7 @@
 #include "elem_body.cuh"
 #include "elem_math.cuh"
 #include "kernels.cuh"
+#include "lulesh_b200.h"
 
 namespace lulesh {
 
@@ -57,6 +58,13 @@ __global__ void k_time_increment(TimeCtl *tcs, int ntc, Params P)
         T.done = 1;
         return;
     }
+#if LULESH_CHECKED
+    if (T.chk != 0) {
+        T.status = LULESH_BOUNDS_ERROR;
+        T.done = 1;
+        return;
+    }
+#endif
     // while (time < stoptime) ... if (its == num_iters) break (lulesh.cu:4858-4873)
     if (!(T.time < P.stoptime) || (T.its_cap > 0 && T.cycle >= T.its_cap)) {
         T.done = 1;
@@ -132,6 +140,8 @@ __global__ void __launch_bounds__(BS, min_blocks(kForceMinBlocks, BS)) k_force(S
     // hourglass step (measured on B200 at -s 100: 150 -> 136 us)
     int n[8];
     elem_nodes<U>(D, elem, n);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) n[i] = chk_index(n[i], D.numNode, &T, kChkNode);
     double xn[8], yn[8], zn[8];
     double xdn[8], ydn[8], zdn[8];
 #pragma unroll
@@ -186,7 +196,7 @@ void launch_force(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int b
 // the undecomposed mesh's sum bit for bit.
 __device__ __forceinline__ void gather_corners(const DomDev *doms, const DomDev &D, int px,
                                                int py, int pz, double &fx, double &fy,
-                                               double &fz)
+                                               double &fz, TimeCtl *T)
 {
     const int nx = D.nx;
     fx = fy = fz = 0.0;
@@ -196,7 +206,8 @@ __device__ __forceinline__ void gather_corners(const DomDev *doms, const DomDev 
         const bool inside = (unsigned)ex < (unsigned)nx && (unsigned)ey < (unsigned)nx &&
                             (unsigned)ez < (unsigned)nx;
         if (inside) {
-            const int idx = j * D.Ep + (ez * nx + ey) * nx + ex;
+            const int idx = chk_index(j * D.Ep + (ez * nx + ey) * nx + ex, 8LL * D.Ep, T,
+                                      kChkCorner);
             fx += ld_corner(D.fx_elem + idx);
             fy += ld_corner(D.fy_elem + idx);
             fz += ld_corner(D.fz_elem + idx);
@@ -208,7 +219,8 @@ __device__ __forceinline__ void gather_corners(const DomDev *doms, const DomDev 
             if (nb >= 0) {
                 const DomDev &N = doms[nb];
                 const int lx = ex - sx * nx, ly = ey - sy * nx, lz = ez - sz * nx;
-                const int idx = j * N.Ep + (lz * nx + ly) * nx + lx;
+                const int idx = chk_index(j * N.Ep + (lz * nx + ly) * nx + lx, 8LL * N.Ep,
+                                          T, kChkCorner);
                 fx += ld_corner(N.fx_elem + idx);
                 fy += ld_corner(N.fy_elem + idx);
                 fz += ld_corner(N.fz_elem + idx);
@@ -282,11 +294,11 @@ __global__ void __launch_bounds__(BS, min_blocks(kNodalMinBlocks, BS)) k_nodal(S
 
     double fx, fy, fz;
     if (MODE == 0) {
-        gather_corners(a.doms, D, px, py, pz, fx, fy, fz);
+        gather_corners(a.doms, D, px, py, pz, fx, fy, fz, &a.tcs[D.tc]);
     } else if (MODE == 1) {
         DomDev L = D;
         L.tp = 1;  // own corners only
-        gather_corners(a.doms, L, px, py, pz, fx, fy, fz);
+        gather_corners(a.doms, L, px, py, pz, fx, fy, fz, &a.tcs[D.tc]);
         D.fx[i] = fx;
         D.fy[i] = fy;
         D.fz[i] = fz;
@@ -322,15 +334,25 @@ __global__ void __launch_bounds__(BS, min_blocks(kNodalUMinBlocks, BS)) k_nodal_
     if (!T.active) return;  // the whole block
     const int first = blk.y;
     const int last = min(first + BS, D.numNode) - 1;
-    const int lo = D.nodeElemStart[first];
+    const long long list_len = 8LL * D.numElem;  // corner-list entries
+    const int lo = chk_index(D.nodeElemStart[first], list_len, const_cast<TimeCtl *>(&T),
+                             kChkCornerRun);
     const int len = D.nodeElemStart[last] + D.nodeElemCount[last] - lo;
-    const bool staged = len <= 8 * BS;
+    const bool staged = len <= 8 * BS && lo + (long long)len <= list_len;
     if (staged)
         for (int k = threadIdx.x; k < len; k += BS) s_list[k] = D.nodeElemCornerList[lo + k];
     __syncthreads();
     const int i = first + threadIdx.x;
     if (i > last) return;
-    const int start = D.nodeElemStart[i], count = D.nodeElemCount[i];
+    int start = D.nodeElemStart[i], count = D.nodeElemCount[i];
+#if LULESH_CHECKED
+    if (start < 0 || count < 0 || start + (long long)count > list_len ||
+        (staged && (start < lo || start + count > lo + len))) {
+        atomicCAS(&const_cast<TimeCtl &>(T).chk, 0, (int)kChkCornerRun);
+        start = lo;
+        count = 0;
+    }
+#endif
     const int *list = staged ? s_list + (start - lo) : D.nodeElemCornerList + start;
 
     double fx = 0.0, fy = 0.0, fz = 0.0;
@@ -339,7 +361,8 @@ __global__ void __launch_bounds__(BS, min_blocks(kNodalUMinBlocks, BS)) k_nodal_
         int k[4];
         double vx[4], vy[4], vz[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) k[q] = list[j + q];
+        for (int q = 0; q < 4; ++q)
+            k[q] = chk_index(list[j + q], 8LL * D.Ep, const_cast<TimeCtl *>(&T), kChkCorner);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             vx[q] = ld_corner(D.fx_elem + k[q]);
@@ -354,7 +377,7 @@ __global__ void __launch_bounds__(BS, min_blocks(kNodalUMinBlocks, BS)) k_nodal_
         }
     }
     for (; j < count; ++j) {
-        const int k = list[j];
+        const int k = chk_index(list[j], 8LL * D.Ep, const_cast<TimeCtl *>(&T), kChkCorner);
         fx += ld_corner(D.fx_elem + k);
         fy += ld_corner(D.fy_elem + k);
         fz += ld_corner(D.fz_elem + k);
@@ -403,6 +426,8 @@ __global__ void __launch_bounds__(BS, min_blocks(kKinMinBlocks, BS)) k_kinematic
     // all node gathers first (measured on B200 at -s 100: 92 -> 84 us)
     int nodes[8];
     elem_nodes<U>(D, k, nodes);
+#pragma unroll
+    for (int l = 0; l < 8; ++l) nodes[l] = chk_index(nodes[l], D.numNode, &T, kChkNode);
     double x_local[8], y_local[8], z_local[8];
     double xd_local[8], yd_local[8], zd_local[8];
 #pragma unroll
@@ -489,7 +514,8 @@ __device__ __forceinline__ void elem_face_links(const DomDev &D, int z, int &bc,
 __device__ __forceinline__ double mono_limiter(const double *delv, int i, int bc, int mmask,
                                                int msymm, int mfree, int pmask, int psymm,
                                                int pfree, int lm, int lp, double mult,
-                                               double maxslope, double ptiny)
+                                               double maxslope, double ptiny, int nlinks,
+                                               TimeCtl *T)
 {
     const double norm = 1. / (delv[i] + ptiny);
     double delvm, delvp;
@@ -498,14 +524,14 @@ __device__ __forceinline__ double mono_limiter(const double *delv, int i, int bc
         delvm = delv[i];
     else if (mb == mfree)
         delvm = 0.0;
-    else
-        delvm = delv[lm];  // 0 or *_COMM: neighbour or ghost element
+    else  // 0 or *_COMM: neighbour or ghost element
+        delvm = delv[chk_index(lm, nlinks, T, kChkLink)];
     if (pb == psymm)
         delvp = delv[i];
     else if (pb == pfree)
         delvp = 0.0;
     else
-        delvp = delv[lp];
+        delvp = delv[chk_index(lp, nlinks, T, kChkLink)];
     delvm = delvm * norm;
     delvp = delvp * norm;
     double phi = .5 * (delvm + delvp);
@@ -617,7 +643,7 @@ __global__ void __launch_bounds__(BS, min_blocks(kEosMinBlocks, BS)) k_eos(SetAr
         // (HostDomain::eosOrder), which keeps the trip count uniform per warp
         // with denser loads (measured 98 us vs 99 us regElemlist order and
         // 108 us natural order at -s 100).
-        const int zidx = D.eosOrder[i];
+        const int zidx = chk_index(D.eosOrder[i], D.numElem, &T, kChkSlot);
         int cls = 0;
         while (cls < D.eosNumClass - 1 && i >= D.eosClassEnd[cls]) ++cls;
         const int rep = D.eosClassRep[cls];
@@ -639,13 +665,13 @@ __global__ void __launch_bounds__(BS, min_blocks(kEosMinBlocks, BS)) k_eos(SetAr
         const double mult = P.monoq_limiter_mult, maxs = P.monoq_max_slope;
         const double phixi =
             mono_limiter(D.delv_xi, zidx, bcMask, XI_M, XI_M_SYMM, XI_M_FREE, XI_P, XI_P_SYMM,
-                         XI_P_FREE, lxm, lxp, mult, maxs, ptiny);
+                         XI_P_FREE, lxm, lxp, mult, maxs, ptiny, D.allElem, &T);
         const double phieta =
             mono_limiter(D.delv_eta, zidx, bcMask, ETA_M, ETA_M_SYMM, ETA_M_FREE, ETA_P,
-                         ETA_P_SYMM, ETA_P_FREE, lem, lep, mult, maxs, ptiny);
+                         ETA_P_SYMM, ETA_P_FREE, lem, lep, mult, maxs, ptiny, D.allElem, &T);
         const double phizeta =
             mono_limiter(D.delv_zeta, zidx, bcMask, ZETA_M, ZETA_M_SYMM, ZETA_M_FREE, ZETA_P,
-                         ZETA_P_SYMM, ZETA_P_FREE, lzm, lzp, mult, maxs, ptiny);
+                         ZETA_P_SYMM, ZETA_P_FREE, lzm, lzp, mult, maxs, ptiny, D.allElem, &T);
         const double vdov_z = D.vdov[zidx];
         const double vnew_z = D.vnew[zidx];
         double qlin, qquad;

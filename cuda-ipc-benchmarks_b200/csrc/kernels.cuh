@@ -78,6 +78,36 @@ struct SetArgs {
 };
 
 // ---------------------------------------------------------------------------
+// checked builds
+//
+// With -DLULESH_CHECKED=1 the FP64 cycle kernels range-check every index
+// they compute or load before using it: node indices, corner indices,
+// corner-list runs, EOS slots and face links.  An index out of range is
+// replaced by 0, which every array holds, so no access leaves its array and
+// no thread leaves the kernel's control flow.  The first failing check's
+// code is kept in TimeCtl::chk, and the next time increment ends the job
+// with LULESH_BOUNDS_ERROR.  This build stands in for a memory checker.
+#ifndef LULESH_CHECKED
+#define LULESH_CHECKED 0
+#endif
+enum CheckCode { kChkNode = 1, kChkCorner = 2, kChkCornerRun = 3, kChkSlot = 4, kChkLink = 5 };
+
+__device__ __forceinline__ int chk_index(long long i, long long n, TimeCtl *T, int code)
+{
+#if LULESH_CHECKED
+    if (i < 0 || i >= n) {
+        atomicCAS(&T->chk, 0, code);
+        return 0;
+    }
+#else
+    (void)n;
+    (void)T;
+    (void)code;
+#endif
+    return (int)i;
+}
+
+// ---------------------------------------------------------------------------
 // programmatic dependent launch
 //
 // The cycle kernels may be launched with programmatic stream serialisation

@@ -49,7 +49,7 @@ struct TimeCtl {
     int bad_vol;     // smallest element index with a volume error, INT_MAX
     int bad_q;       // smallest element index with q > qstop, INT_MAX
     int status;      // lulesh_status of the job
-    int pad;
+    int chk;         // checked builds: code of the first index out of range, 0 none
 };
 
 // One domain.  Sizes follow lulesh.cu:783-798; node (px,py,pz) has index

@@ -470,6 +470,7 @@ const char *lulesh_status_string(int st)
         case LULESH_OOM: return "out of device memory";
         case LULESH_TIMEOUT: return "timeout";
         case LULESH_NO_DEVICE: return "no CUDA device";
+        case LULESH_BOUNDS_ERROR: return "index out of range (checked build)";
         default: return "unknown status";
     }
 }

@@ -25,6 +25,7 @@ INVALID_ARG = -5
 OOM = -6
 TIMEOUT = -7
 NO_DEVICE = -8
+BOUNDS_ERROR = -9  # -DLULESH_CHECKED builds only
 
 FLAG_MATERIALIZE = 0x1
 FLAG_COMM_STAGED = 0x2

@@ -45,7 +45,9 @@ enum lulesh_status {
     LULESH_INVALID_ARG = -5,  /* bad argument (size, index, name, ...)  */
     LULESH_OOM = -6,          /* device memory exhausted / over the cap */
     LULESH_TIMEOUT = -7,      /* a bounded device wait gave up          */
-    LULESH_NO_DEVICE = -8     /* no CUDA device / extension unusable    */
+    LULESH_NO_DEVICE = -8,    /* no CUDA device / extension unusable    */
+    LULESH_BOUNDS_ERROR = -9  /* -DLULESH_CHECKED builds only: a kernel
+                                 index was out of range (replaced by 0) */
 };
 
 /* create flags */

@@ -31,6 +31,17 @@ def test_every_declared_symbol_is_exported(lulesh):
     assert declared <= set(lulesh.EXPORTED), declared - set(lulesh.EXPORTED)
 
 
+def test_checked_build_exports_the_same_symbols(lulesh):
+    """liblulesh_b200_checked.so (-DLULESH_CHECKED=1) is a drop-in for the
+    normal library: same symbols, and the bounds status has its name."""
+    path = os.path.join(REPO, "cuda-ipc-benchmarks_b200", "liblulesh_b200_checked.so")
+    assert os.path.exists(path), "build it with make -C cuda-ipc-benchmarks_b200"
+    lib = lulesh.load_library(path)
+    missing = [n for n in sorted(_declared()) if not hasattr(lib, n)]
+    assert not missing, missing
+    assert lib.lulesh_status_string(lulesh.BOUNDS_ERROR).startswith(b"index out of range")
+
+
 def test_status_strings_without_device(lulesh):
     lib = lulesh.load_library()
     assert lib.lulesh_status_string(-1) == b"VolumeError"
