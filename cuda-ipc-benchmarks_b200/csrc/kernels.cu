@@ -845,7 +845,8 @@ __global__ void k_posvel_sync(SetArgs a)
     const int nb = D.nbr[(sx + 1) + 3 * (sy + 1) + 9 * (sz + 1)];
     if (nb < 0) return;
     const DomDev &O = a.doms[nb];
-    const int j = ((pz - sz * nx) * en + (py - sy * nx)) * en + (px - sx * nx);
+    const int j = chk_index(((pz - sz * nx) * en + (py - sy * nx)) * en + (px - sx * nx),
+                            O.numNode, &a.tcs[D.tc], kChkNode);
     D.x[i] = O.x[j];
     D.y[i] = O.y[j];
     D.z[i] = O.z[j];
@@ -886,7 +887,8 @@ __global__ void k_monoq_ghost(SetArgs a)
     const int nb = D.nbr[(dxn + 1) + 3 * (dyn + 1) + 9 * (dzn + 1)];
     if (nb < 0) return;
     const DomDev &N = a.doms[nb];
-    const int g = D.ghost[f] + item;
+    const int g = chk_index(D.ghost[f] + item, D.allElem, &a.tcs[D.tc], kChkLink);
+    src = chk_index(src, N.numElem, &a.tcs[D.tc], kChkLink);
     D.delv_xi[g] = N.delv_xi[src];
     D.delv_eta[g] = N.delv_eta[src];
     D.delv_zeta[g] = N.delv_zeta[src];

@@ -61,6 +61,8 @@ __global__ void __launch_bounds__(kElemBlock, LULESH_MIXED_FORCE_MINB)
 
     int n[8];
     elem_nodes_m(D, elem, n);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) n[i] = chk_index(n[i], D.numNode, &T, kChkNode);
     // all node gathers first: the velocities arrive while the coordinate
     // arithmetic runs
     float vx[8], vy[8], vz[8];
@@ -159,7 +161,8 @@ __global__ void __launch_bounds__(kNodeBlock, min_blocks(kNodalMinBlocks, kNodeB
         const int ex = px - ox[j], ey = py - oy[j], ez = pz - oz[j];
         if ((unsigned)ex < (unsigned)nx && (unsigned)ey < (unsigned)nx &&
             (unsigned)ez < (unsigned)nx) {
-            const int idx = j * D.Ep + (ez * nx + ey) * nx + ex;
+            const int idx = chk_index(j * D.Ep + (ez * nx + ey) * nx + ex, 8LL * D.Ep,
+                                      &a.tcs[D.tc], kChkCorner);
             comp_add(sx, cx, __ldcs(cf.fx + idx));
             comp_add(sy, cy, __ldcs(cf.fy + idx));
             comp_add(sz, cz, __ldcs(cf.fz + idx));
@@ -214,6 +217,8 @@ __global__ void __launch_bounds__(kElemBlock, LULESH_MIXED_KIN_MINB)
     if (k >= D.numElem) return;
     int nodes[8];
     elem_nodes_m(D, k, nodes);
+#pragma unroll
+    for (int l = 0; l < 8; ++l) nodes[l] = chk_index(nodes[l], D.numNode, &T, kChkNode);
     // velocities gathered first (used after the FP64 volume)
     float xv[8], yv[8], zv[8];
 #pragma unroll

@@ -33,6 +33,8 @@ def run(tmpdir):
     for nx, its in ((1, -1), (5, -1), (12, 40)):
         with L.LuleshSet(nx=nx, its=its) as s:
             record(f"single_{nx}", s)
+    with L.LuleshSet(nx=12, its=40, flags=L.FLAG_MIXED) as s:
+        record("mixed", s)
     for flags, name in ((0, "fused"), (L.FLAG_COMM_STAGED, "staged")):
         with L.LuleshSet(nx=6, tp=2, its=30, flags=flags) as s:
             record(f"subdomains_{name}", s, ndom=8)
