@@ -176,9 +176,14 @@ __global__ void k_pack(const DomDev *doms, const TimeCtl *tcs, const Msg *msgs,
     const int item = b.y + threadIdx.x;
     if (item >= m.count) return;
     const DomDev &R = doms[m.dst];
-    const int src = msg_source_index(S, m, item, elems != 0);
-    double *dst = R.commRecv + m.recv_off + item;
-    for (int f = 0; f < fl.n; ++f) dst[(long)f * m.count] = field_ptr(S, fl.id[f])[src];
+    TimeCtl *T = const_cast<TimeCtl *>(&tcs[R.tc]);
+    const int src = chk_index(msg_source_index(S, m, item, elems != 0),
+                              elems ? S.numElem : S.numNode, T, kChkNode);
+    for (int f = 0; f < fl.n; ++f) {
+        const int d = chk_index(m.recv_off + item + (long long)f * m.count, R.commRecvLen, T,
+                                kChkLink);
+        R.commRecv[d] = field_ptr(S, fl.id[f])[src];
+    }
 }
 
 // ---- unpack: CommSBNGpu / CommSyncPosVelGpu ---------------------------------
@@ -239,9 +244,10 @@ __global__ void k_unpack_nodes(const DomDev *doms, const TimeCtl *tcs, const int
         }
         if (!cover) continue;
         touched = true;
-        const double *msg = R.commRecv + off + item;
         for (int f = 0; f < fl.n; ++f) {
-            const double v = msg[(long)f * count];
+            const double v = R.commRecv[chk_index(off + item + (long long)f * count,
+                                                  R.commRecvLen,
+                                                  const_cast<TimeCtl *>(&tcs[R.tc]), kChkLink)];
             acc[f] = add ? acc[f] + v : v;
         }
     }
@@ -273,10 +279,12 @@ __global__ void k_unpack_monoq(const DomDev *doms, const TimeCtl *tcs, const int
         if (R.ghost[k] >= 0) ++pmsg;
     const long off = (long)pmsg * 3 * maxPlane;
     const int count = nx * nx;
-    const int g = R.ghost[f] + item;
-    R.delv_xi[g] = R.commRecv[off + item];
-    R.delv_eta[g] = R.commRecv[off + count + item];
-    R.delv_zeta[g] = R.commRecv[off + 2 * count + item];
+    TimeCtl *T = const_cast<TimeCtl *>(&tcs[R.tc]);
+    const int g = chk_index(R.ghost[f] + item, R.allElem, T, kChkLink);
+    const long long len = R.commRecvLen;
+    R.delv_xi[g] = R.commRecv[chk_index(off + item, len, T, kChkLink)];
+    R.delv_eta[g] = R.commRecv[chk_index(off + count + item, len, T, kChkLink)];
+    R.delv_zeta[g] = R.commRecv[chk_index(off + 2 * count + item, len, T, kChkLink)];
 }
 
 // ---- host side --------------------------------------------------------------
