@@ -124,17 +124,10 @@ __device__ __constant__ int kCZ[8] = {0, 0, 0, 0, 1, 1, 1, 1};
 // ---------------------------------------------------------------------------
 // force: CalcVolumeForceForElems_kernel, lulesh.cu:2080-2259
 
-template <bool HG, int BS, bool U>
-__global__ void __launch_bounds__(BS, min_blocks(kForceMinBlocks, BS)) k_force(SetArgs a, Params P)
+// one element of the force phase: the node gathers, then force_elem
+template <bool HG, bool U>
+__device__ __forceinline__ void force_one(const DomDev &D, TimeCtl &T, const Params &P, int elem)
 {
-    pdl_enter();
-    const int2 blk = a.blocks[LULESH_FORCE_REVERSE ? gridDim.x - 1 - blockIdx.x : blockIdx.x];
-    const DomDev &D = a.doms[blk.x];
-    TimeCtl &T = a.tcs[D.tc];
-    if (!T.active) return;
-    const int elem = blk.y + threadIdx.x;
-    if (elem >= D.numElem) return;
-
     // all 48 node gathers are issued before any arithmetic: the velocity
     // loads then overlap the coordinate work instead of stalling the
     // hourglass step (measured on B200 at -s 100: 150 -> 136 us)
@@ -162,6 +155,19 @@ __global__ void __launch_bounds__(BS, min_blocks(kForceMinBlocks, BS)) k_force(S
 #pragma unroll
     for (int i = 0; i < 8; ++i) zn[i] = D.z[n[i]];
     force_elem<HG>(D, T, P, elem, xn, yn, zn, vel);
+}
+
+template <bool HG, int BS, bool U>
+__global__ void __launch_bounds__(BS, min_blocks(kForceMinBlocks, BS)) k_force(SetArgs a, Params P)
+{
+    pdl_enter();
+    const int2 blk = a.blocks[LULESH_FORCE_REVERSE ? gridDim.x - 1 - blockIdx.x : blockIdx.x];
+    const DomDev &D = a.doms[blk.x];
+    TimeCtl &T = a.tcs[D.tc];
+    if (!T.active) return;
+    const int elem = blk.y + threadIdx.x;
+    if (elem >= D.numElem) return;
+    force_one<HG, U>(D, T, P, elem);
 }
 
 template <int BS, bool U = false>
