@@ -35,6 +35,7 @@ DomSizes sizes_of(const HostDomain &h, long comm_doubles)
     s.nr = (size_t)h.numReg;
     s.comm = 0;
     s.unstructured = true;
+    s.ell = !h.nodeCornerEll.empty();
     return s;
 }
 
@@ -56,6 +57,7 @@ size_t domain_bytes(const DomSizes &s, bool mixed)
     if (s.comm) b += align256(8 * s.comm);
     if (mixed) b += 3 * align256(4 * 8 * s.Ep);
     if (s.unstructured) b += align256(4 * s.N);  // nodeBC
+    if (s.ell) b += align256(4 * 8 * s.N);       // nodeCornerEll
     return b;
 }
 
@@ -148,6 +150,7 @@ int upload_domain(const HostDomain &h, int tc, long comm_doubles, bool mixed, Ca
     D.unstructured = h.unstructured ? 1 : 0;
     D.octant = h.octantCorner;
     if (h.unstructured) D.nodeBC = cv.take<int>(z.N);
+    if (z.ell) D.nodeCornerEll = cv.take<int>(8 * z.N);
     if (mixed && c32) {
         c32->fx = cv.take<float>(8 * z.Ep);
         c32->fy = cv.take<float>(8 * z.Ep);
@@ -205,6 +208,7 @@ int upload_domain(const HostDomain &h, int tc, long comm_doubles, bool mixed, Ca
     for (size_t k = 0; k < sizeof(ip) / sizeof(ip[0]); ++k)
         if ((su = upload(ip[k], *iv[k], st)) != LULESH_OK) return su;
     if (h.unstructured && (su = upload(D.nodeBC, h.nodeBC, st)) != LULESH_OK) return su;
+    if (z.ell && (su = upload(D.nodeCornerEll, h.nodeCornerEll, st)) != LULESH_OK) return su;
     // the host vectors must outlive the asynchronous copies
     DCHECK(cudaStreamSynchronize(st));
     *out = D;

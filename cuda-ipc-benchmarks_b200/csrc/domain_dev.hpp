@@ -14,6 +14,7 @@ namespace lulesh {
 struct DomSizes {
     size_t E, N, Ep, allElem, corner, en2, nr, comm;
     bool unstructured = false;  // adds the per-node boundary mask
+    bool ell = false;           // adds the slot-major corner runs (8 per node)
 };
 
 DomSizes sizes_of(int nx, int numReg, long comm_doubles);

@@ -613,6 +613,14 @@ bool build_domain_lmesh(HostDomain &d, const char *path, int numReg, int balance
                XI_P_FREE, d.elemBC);
 
     build_corner_csr(d);
+    // the corner runs again, slot-major, for the nodal kernel's coalesced
+    // reads (meshes where no node has more than 8 corners)
+    if (*std::max_element(d.nodeElemCount.begin(), d.nodeElemCount.end()) <= 8) {
+        d.nodeCornerEll.assign((size_t)8 * N, -1);
+        for (int n = 0; n < N; ++n)
+            for (int j = 0; j < d.nodeElemCount[n]; ++j)
+                d.nodeCornerEll[(size_t)j * N + n] = d.nodeElemCornerList[d.nodeElemStart[n] + j];
+    }
     d.matElemlist.resize(E);
     for (int z = 0; z < E; ++z) d.matElemlist[z] = z;
     d.volo.resize(E);

@@ -55,6 +55,9 @@ struct HostDomain {
     bool unstructured = false;
     int octantCorner = 0;
     std::vector<int> nodeBC;  // per node: bit 0/1/2 = in symmX/Y/Z
+    // when no node has more than 8 corners: slot j of node i's corner run at
+    // [j * numNode + i], -1 past the run (empty otherwise)
+    std::vector<int> nodeCornerEll;
 };
 
 // Reference parameter block, lulesh.cu:1125-1158.

@@ -340,6 +340,41 @@ __global__ void __launch_bounds__(BS, min_blocks(kNodalUMinBlocks, BS)) k_nodal_
     if (!T.active) return;  // the whole block
     const int first = blk.y;
     const int last = min(first + BS, D.numNode) - 1;
+    if (D.nodeCornerEll) {
+        // the run slot-major (uniform per block: no staging, no barrier):
+        // eight coalesced loads, then the corners, summed in run order
+        const int i = first + threadIdx.x;
+        if (i > last) return;
+        const int N = D.numNode;
+        int k[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) k[j] = D.nodeCornerEll[(size_t)j * N + i];
+        double fx = 0.0, fy = 0.0, fz = 0.0;
+#pragma unroll
+        for (int h = 0; h < 8; h += 4) {
+            double vx[4], vy[4], vz[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                vx[q] = vy[q] = vz[q] = 0.0;
+                if (k[h + q] >= 0) {
+                    const int c = chk_index(k[h + q], 8LL * D.Ep, const_cast<TimeCtl *>(&T),
+                                            kChkCorner);
+                    vx[q] = ld_corner(D.fx_elem + c);
+                    vy[q] = ld_corner(D.fy_elem + c);
+                    vz[q] = ld_corner(D.fz_elem + c);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (k[h + q] >= 0) {  // a run is a prefix of the slots
+                    fx += vx[q];
+                    fy += vy[q];
+                    fz += vz[q];
+                }
+        }
+        advance_node(D, T, P, i, D.nodeBC[i], fx, fy, fz, a.materialize, true);
+        return;
+    }
     const long long list_len = 8LL * D.numElem;  // corner-list entries
     const int lo = chk_index(D.nodeElemStart[first], list_len, const_cast<TimeCtl *>(&T),
                              kChkCornerRun);

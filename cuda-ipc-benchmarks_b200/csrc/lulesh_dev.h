@@ -89,6 +89,10 @@ struct DomDev {
     int unstructured;
     int octant;  // element holding the energy deposit (0 on -s meshes)
     int *nodeBC;
+    // slot j of node i's corner run at [j * numNode + i], -1 past the run;
+    // null when some node has more than 8 corners (the kernel then reads the
+    // run from nodeElemCornerList)
+    int *nodeCornerEll;
 };
 
 // Mixed-precision corner forces, FP32, layout of fx_elem ([8][Ep]).
