@@ -31,7 +31,7 @@ static long copy_field(const lulesh::HostDomain &d, const char *name, void *out,
                 {"regElemSize", &d.regElemSize}, {"regCSR", &d.regCSR},
                 {"regReps", &d.regReps}, {"regNumList", &d.regNumList},
                 {"regElemlist", &d.regElemlist}, {"regSorted", &d.regSorted},
-                {"nodeBC", &d.nodeBC}};
+                {"nodeBC", &d.nodeBC}, {"nodeCornerEll", &d.nodeCornerEll}};
     struct R {
         const char *n;
         const std::vector<double> *v;

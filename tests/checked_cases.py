@@ -10,6 +10,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 sys.path.insert(0, os.path.join(REPO, "cuda-ipc-benchmarks_b200"))
 
+import numpy as np  # noqa: E402
+
 import lmesh  # noqa: E402
 import lulesh_b200 as L  # noqa: E402
 
@@ -46,6 +48,17 @@ def run(tmpdir):
     lmesh.write(path, lmesh.warp(m))
     with L.LuleshSet.from_mesh(path) as s:
         record("unstructured", s)
+    # nodes with more than 8 corners (duplicated elements): the staged and
+    # the list-reading corner-run paths of the unstructured nodal kernel
+    for name, nx, dup in (("dup_one", 8, [200]), ("dup_all", 6, None)):
+        b = lmesh.box(nx)
+        idx = list(range(b.num_elem)) if dup is None else dup
+        d = lmesh.LMesh(b.xyz, np.concatenate([b.nodelist, b.nodelist[idx]]),
+                        np.concatenate([b.links, b.links[idx]]), b.symm, b.free)
+        path = os.path.join(tmpdir, name + ".lmesh")
+        lmesh.write(path, d)
+        with L.LuleshSet.from_mesh(path) as s:
+            record(name, s)
     return out
 
 

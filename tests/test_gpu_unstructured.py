@@ -114,6 +114,17 @@ def test_element_renumbering(lulesh, tmp_path):
     assert np.abs(x_a - x_b).max() <= 1e-12
 
 
+def duplicated(m, elems):
+    """The mesh with copies of the listed elements appended: the copies share
+    their originals' nodes and face links, so those nodes gain corners (a
+    node of a duplicated interior element has up to 16).  Physically it is
+    a denser material there; arithmetically it is a valid mesh, and it takes
+    the nodal kernel off its at-most-8-corners path."""
+    elems = np.asarray(elems, dtype=np.int64)
+    return lmesh.LMesh(m.xyz.copy(), np.concatenate([m.nodelist, m.nodelist[elems]]),
+                       np.concatenate([m.links, m.links[elems]]), m.symm, m.free)
+
+
 def _compare(s, o, fields, E, N, rtol, atol=1e-14):
     """Max difference relative to the field's largest magnitude; a field
     that is still ~0 everywhere (delv after one cycle: the last bit of a
@@ -129,13 +140,23 @@ def _compare(s, o, fields, E, N, rtol, atol=1e-14):
     return bad
 
 
-@pytest.mark.parametrize("mesh", ["warped", "sedov15oct"])
+@pytest.mark.parametrize("mesh", ["warped", "sedov15oct", "dup_one", "dup_all"])
 def test_matches_oracle(lulesh, oracle_mod, tmp_path, mesh):
     """Against the CPU oracle's reading of the same file: a curvilinear,
-    renumbered -s 10 box (generated here), and the reference's own octant
-    mesh when its copy is present.  One cycle to rounding level, then the
-    full run to t = 0.01: same cycle count, origin energy within 1e-9."""
-    if mesh == "warped":
+    renumbered -s 10 box (generated here), the reference's own octant mesh
+    when its copy is present, and boxes with duplicated elements whose nodes
+    have more than 8 corners (one duplicate: the staged corner-run path; all
+    duplicated: runs too long to stage, read from the list).  One cycle to
+    rounding level, then the full run to t = 0.01: same cycle count, origin
+    energy within 1e-9."""
+    if mesh == "dup_one":
+        path = str(tmp_path / "dup_one.lmesh")
+        lmesh.write(path, duplicated(lmesh.box(8), [200]))
+    elif mesh == "dup_all":
+        m = lmesh.box(6)
+        path = str(tmp_path / "dup_all.lmesh")
+        lmesh.write(path, duplicated(m, np.arange(m.num_elem)))
+    elif mesh == "warped":
         m = lmesh.box(10)
         rng = np.random.default_rng(3)
         path = str(tmp_path / "warped.lmesh")

@@ -105,7 +105,8 @@ def _host_lmesh(path, name):
                   ctypes.c_void_p, ctypes.c_long]
     n = f(str(path).encode(), 11, 1, 1, name.encode(), None, 0)
     assert n >= 0, (name, n)
-    dt = np.int32 if name in INT_FIELDS or name == "octant" else np.float64
+    ints = INT_FIELDS | {"octant", "nodeCornerEll", "nodeBC"}
+    dt = np.int32 if name in ints else np.float64
     out = np.empty(n, dtype=dt)
     f(str(path).encode(), 11, 1, 1, name.encode(), out.ctypes.data_as(ctypes.c_void_p), n)
     return out
@@ -159,3 +160,22 @@ def test_product_reader_rejects_malformed_files(tmp_path):
     lmesh.write(p, m)
     assert f(str(p).encode(), 11, 1, 1, b"x", None, 0) == -2
     assert f(str(tmp_path / "none.lmesh").encode(), 11, 1, 1, b"x", None, 0) == -2
+
+
+def test_slot_major_runs_only_up_to_8_corners(tmp_path):
+    """The reader lays the corner runs out slot-major (slot j of node i at
+    j * N + i, -1 past the run) when no node has more than 8 corners, and
+    leaves them out otherwise."""
+    p = tmp_path / "b4.lmesh"
+    m = lmesh.box(4)
+    lmesh.write(p, m)
+    ell = _host_lmesh(p, "nodeCornerEll").reshape(8, m.num_node)
+    start, count = _host_lmesh(p, "nodeElemStart"), _host_lmesh(p, "nodeElemCount")
+    runs = _host_lmesh(p, "nodeElemCornerList")
+    for n in range(m.num_node):
+        want = list(runs[start[n]:start[n] + count[n]]) + [-1] * (8 - count[n])
+        assert list(ell[:, n]) == want
+    q = tmp_path / "dup.lmesh"
+    lmesh.write(q, lmesh.LMesh(m.xyz, np.concatenate([m.nodelist, m.nodelist[:1]]),
+                               np.concatenate([m.links, m.links[:1]]), m.symm, m.free))
+    assert _host_lmesh(q, "nodeCornerEll").size == 0
