@@ -681,4 +681,24 @@ void build_domain_light(HostDomain &d, int nx, int numReg, int balance, int cost
     build_regions(d, numReg, balance);
 }
 
+double origin_deltatime(int nx, int tp)
+{
+    // the origin domain's volo[0] and einit, as build_domain computes them
+    const int meshEdge = nx * tp;
+    double xl[8], yl[8], zl[8];
+    const int dx[8] = {0, 1, 1, 0, 0, 1, 1, 0};
+    const int dy[8] = {0, 0, 1, 1, 0, 0, 1, 1};
+    const int dz[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+    for (int k = 0; k < 8; ++k) {
+        xl[k] = lattice(dx[k], meshEdge);
+        yl[k] = lattice(dy[k], meshEdge);
+        zl[k] = lattice(dz[k], meshEdge);
+    }
+    const double volo0 = elem_volume_host(xl, yl, zl);
+    const double ebase = 3.948746e+7;
+    double scale = (nx * tp) / 45.0;
+    const double einit = ebase * scale * scale * scale;
+    return (.5 * cbrt(volo0)) / sqrt(2 * einit);
+}
+
 }  // namespace lulesh

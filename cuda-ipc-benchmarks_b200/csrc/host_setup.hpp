@@ -92,6 +92,11 @@ void build_domain_light(HostDomain &d, int nx, int numReg, int balance, int cost
 bool build_domain_lmesh(HostDomain &d, const char *path, int numReg, int balance, int cost,
                         std::string *err);
 
+// The initial dt of a tp^3 problem of nx^3 subdomains: that of the domain
+// holding the origin (lulesh.cu:1189-1205), which every subdomain starts
+// from.
+double origin_deltatime(int nx, int tp);
+
 // CalcElemVolume (lulesh.cu:221-307), host copy used at setup.
 double elem_volume_host(const double *x, const double *y, const double *z);
 

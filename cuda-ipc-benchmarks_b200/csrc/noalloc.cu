@@ -14,8 +14,9 @@
 // The corner forces of up to kNoAllocMaxElems elements live in that array;
 // its last 256 bytes hold the volume-error flag.  Host code never uses the
 // array's name as an address: the device address comes from
-// cudaGetSymbolAddress, looked up once per device, with that device
-// current, on the first call made on it.
+// cudaGetSymbolAddress, looked up with the device current on every call made
+// outside stream capture (a device reset or a caller-created context moves
+// the array), and taken from the last such call while a stream captures.
 #include <climits>
 #include <mutex>
 #include <string>
@@ -35,7 +36,7 @@ constexpr int kBlock = 128;
 static __device__ __align__(256) double g_noalloc_scratch[kCornerDoubles + 32];
 
 std::mutex g_mu;
-void *g_addr[64];  // device address of g_noalloc_scratch, per device ordinal
+void *g_addr[64];  // last looked-up address of g_noalloc_scratch, per device ordinal
 
 __global__ void k_flag_reset(int *flag) { *flag = INT_MAX; }
 
@@ -138,18 +139,33 @@ __global__ void __launch_bounds__(kBlock)
     fz[i] = sz;
 }
 
-// Device address of the scratch array for the current device, looked up
-// on the first call made on that device.
-int scratch_address(void **out)
+// Device address of the scratch array in the current context, for a call
+// enqueued on stream s.  Outside stream capture every call looks it up
+// (cudaGetSymbolAddress, with the caller's device current; a host-side
+// table lookup once the module is loaded), so the address is always that of
+// the current context: after cudaDeviceReset the module is loaded again and
+// the array may sit at a new address, and a context the caller created
+// holds its own copy.  While s is capturing, the address of the last call
+// on this device outside capture is used; with none, the call is refused.
+int scratch_address(cudaStream_t s, void **out)
 {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return LULESH_NO_DEVICE;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) {
+        (void)cudaGetLastError();
+        cs = cudaStreamCaptureStatusActive;  // treat an unclear answer as capture
+    }
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_addr[dev]) {
+    if (cs == cudaStreamCaptureStatusNone) {
         void *ptr = nullptr;
         if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr)
             return LULESH_CUDA_ERROR;
         g_addr[dev] = ptr;
+    } else if (!g_addr[dev]) {
+        lulesh::set_error("lulesh_volume_force_noalloc: the first call on a device must come "
+                          "before any stream capture");
+        return LULESH_INVALID_ARG;
     }
     *out = g_addr[dev];
     return LULESH_OK;
@@ -176,12 +192,12 @@ extern "C" int lulesh_volume_force_noalloc(int nx, const double *x, const double
         lulesh::set_error("lulesh_volume_force_noalloc: null array argument");
         return LULESH_INVALID_ARG;
     }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
     void *base = nullptr;
-    int st = scratch_address(&base);
+    int st = scratch_address(s, &base);
     if (st != LULESH_OK) return st;
     double *corners = static_cast<double *>(base);
     int *flag = reinterpret_cast<int *>(corners + kCornerDoubles);
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int numElem = nx * nx * nx, numNode = (nx + 1) * (nx + 1) * (nx + 1);
     k_flag_reset<<<1, 1, 0, s>>>(flag);
     if (hgcoef > 0.0)

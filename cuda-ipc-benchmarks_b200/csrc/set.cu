@@ -9,6 +9,7 @@
 #include <string>
 
 #include "domain_dev.hpp"
+#include "halo_plan.hpp"
 #include "set.hpp"
 
 namespace lulesh {
@@ -157,8 +158,11 @@ static int create_common(lulesh_set *s, const std::vector<DomPlace> &place, int 
         else if (pl.tp == 1 && !(s->flags & LULESH_FLAG_HOST_SETUP))
             build_domain_light(h, j.nx, j.numReg, j.balance, j.cost);
         else
+            // subdomains: the nodal mass over the whole problem is summed on
+            // the device (nodal_mass_on_device) unless the host builds it all
             build_domain(h, j.nx, pl.tp, pl.col, pl.row, pl.plane, pl.rank, j.numReg, j.balance,
-                         j.cost, /*global_mass=*/pl.tp > 1);
+                         j.cost,
+                         /*global_mass=*/pl.tp > 1 && (s->flags & LULESH_FLAG_HOST_SETUP));
         DomDev D{};
         int su = upload_domain(h, pl.job, commd[d], mixed, cv, s->stream, &D, &hc32[d]);
         if (su != LULESH_OK) return su;
@@ -170,11 +174,27 @@ static int create_common(lulesh_set *s, const std::vector<DomPlace> &place, int 
             job_dt[pl.job] = h.deltatime;  // the origin domain's initial dt
         }
     }
-    // neighbour tables of subdomain sets (rank = col + tp*(row + tp*plane))
+    // a part of a problem split over GPUs: the job's dt starts from the
+    // origin domain's even where that domain lives on another part
+    for (int j = 0; j < s->njobs; ++j)
+        if (s->job_origin[j] < 0) job_dt[j] = origin_deltatime(s->jobs[j].nx, s->tp);
+    // proxies of the neighbours held by other parts, and the halo tables
+    if (s->nparts > 1) {
+        const int pst = part_build(s);
+        if (pst != LULESH_OK) return pst;
+    }
+    // neighbour tables of subdomain sets (rank = col + tp*(row + tp*plane)):
+    // a local neighbour of rank r is domain r - first_rank, a remote one
+    // its proxy
+    auto index_of_rank = [s](int r) -> int {
+        if (halo_part_of(r, s->tp, s->nparts) == s->part) return r - s->first_rank;
+        for (size_t k = 0; k < s->proxy_rank.size(); ++k)
+            if (s->proxy_rank[k] == r) return s->ndom + (int)k;
+        return -1;
+    };
     for (int d = 0; d < s->ndom; ++d) {
         DomDev &D = s->hdoms[d];
         if (D.tp <= 1) continue;
-        const int base = d - s->dom_rank[d];
         for (int dz = -1; dz <= 1; ++dz)
             for (int dy = -1; dy <= 1; ++dy)
                 for (int dx = -1; dx <= 1; ++dx) {
@@ -182,13 +202,18 @@ static int create_common(lulesh_set *s, const std::vector<DomPlace> &place, int 
                     int nbr = -1;
                     if (c >= 0 && r >= 0 && p >= 0 && c < D.tp && r < D.tp && p < D.tp &&
                         !(dx == 0 && dy == 0 && dz == 0))
-                        nbr = base + c + D.tp * (r + D.tp * p);
+                        nbr = index_of_rank(c + D.tp * (r + D.tp * p));
                     D.nbr[(dx + 1) + 3 * (dy + 1) + 9 * (dz + 1)] = nbr;
                 }
     }
-    LCHECK(cudaMalloc(&s->ddoms, sizeof(DomDev) * s->ndom));
+    const size_t ntab = s->hdoms.size() + s->hproxies.size();
+    LCHECK(cudaMalloc(&s->ddoms, sizeof(DomDev) * ntab));
     LCHECK(cudaMemcpyAsync(s->ddoms, s->hdoms.data(), sizeof(DomDev) * s->ndom,
                            cudaMemcpyHostToDevice, s->stream));
+    if (!s->hproxies.empty())
+        LCHECK(cudaMemcpyAsync(s->ddoms + s->ndom, s->hproxies.data(),
+                               sizeof(DomDev) * s->hproxies.size(), cudaMemcpyHostToDevice,
+                               s->stream));
     if (mixed)
         LCHECK(cudaMemcpyAsync(s->dcorner32, hc32.data(), sizeof(CornerF32) * s->ndom,
                                cudaMemcpyHostToDevice, s->stream));
@@ -202,6 +227,16 @@ static int create_common(lulesh_set *s, const std::vector<DomPlace> &place, int 
                            cudaMemcpyHostToDevice, s->stream));
     int st = build_tables(s);
     if (st != LULESH_OK) return st;
+    // subdomains: the init-time nodal mass exchange (lulesh.cu:4811-4831)
+    // as a gather over the neighbours, on the device; a part of several
+    // GPUs does it once its proxies hold the neighbours' volumes
+    if (s->tp > 1 && !(s->flags & LULESH_FLAG_HOST_SETUP)) {
+        if (s->nparts > 1) {
+            s->mass_pending = true;
+        } else if ((st = nodal_mass_on_device(s)) != LULESH_OK) {
+            return st;
+        }
+    }
     LCHECK(cudaStreamSynchronize(s->stream));
     return LULESH_OK;
 }
@@ -290,6 +325,10 @@ static void clear_l2_window(lulesh_set *s)
 static int ensure_graph(lulesh_set *s)
 {
     if (s->graph_ready) return LULESH_OK;
+    if (s->nparts > 1) {
+        set_error("a part of a multi-GPU problem has no one-GPU cycle graph");
+        return LULESH_INVALID_ARG;
+    }
     const int pst = prepare_capture(s);
     if (pst != LULESH_OK) return pst;
     LCHECK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
@@ -525,6 +564,46 @@ int lulesh_create(const lulesh_job *job, int tp, int flags, int device, lulesh_s
     return LULESH_OK;
 }
 
+int lulesh_create_part(const lulesh_job *job, int tp, int nparts, int part, int flags,
+                       int device, lulesh_set **out)
+{
+    if (!job || !out || tp < 1 || tp > 16 || nparts < 1 || nparts > tp * tp * tp || part < 0 ||
+        part >= nparts) {
+        set_error("lulesh_create_part: bad arguments (1 <= nparts <= tp^3, 0 <= part < nparts)");
+        return LULESH_INVALID_ARG;
+    }
+    *out = nullptr;
+    if (nparts == 1) return lulesh_create(job, tp, flags, device, out);
+    int st = validate_job(*job);
+    if (st != LULESH_OK) return st;
+    if (flags & (LULESH_FLAG_MIXED | LULESH_FLAG_COMM_STAGED)) {
+        set_error("a part of a multi-GPU problem runs FP64 with the fused exchange");
+        return LULESH_INVALID_ARG;
+    }
+    lulesh_set *s = new lulesh_set;
+    s->flags = flags;
+    s->tp = tp;
+    s->njobs = 1;
+    s->nparts = nparts;
+    s->part = part;
+    s->jobs.push_back(*job);
+    // this part's run of consecutive ranks (halo_part_of)
+    std::vector<DomPlace> place;
+    s->first_rank = -1;
+    for (int r = 0; r < tp * tp * tp; ++r) {
+        if (halo_part_of(r, tp, nparts) != part) continue;
+        if (s->first_rank < 0) s->first_rank = r;
+        place.push_back(DomPlace{0, tp, r % tp, (r / tp) % tp, r / (tp * tp), r});
+    }
+    st = create_common(s, place, device);
+    if (st != LULESH_OK) {
+        lulesh_destroy(s);
+        return st;
+    }
+    *out = s;
+    return LULESH_OK;
+}
+
 int lulesh_create_batch(const lulesh_job *jobs, int njobs, int flags, int device,
                         lulesh_set **out)
 {
@@ -596,6 +675,7 @@ int lulesh_destroy(lulesh_set *s)
     drop_graph(s);
     clear_l2_window(s);
     comm_release(s);
+    part_release(s);
     if (s->elem_blocks) cudaFree(s->elem_blocks);
     if (s->ddoms) cudaFree(s->ddoms);
     if (s->dtc) cudaFree(s->dtc);
@@ -630,6 +710,11 @@ int lulesh_lagrange_leapfrog(lulesh_set *s) { return lulesh_step(s, 1); }
 int lulesh_step(lulesh_set *s, int ncycles)
 {
     if (!s || ncycles < 0) return LULESH_INVALID_ARG;
+    if (s->nparts > 1) {
+        set_error("a part of a multi-GPU problem advances through lulesh_part_phase and the "
+                  "halo exchange");
+        return LULESH_INVALID_ARG;
+    }
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     LCHECK(cudaStreamIsCapturing(s->stream, &cs));
     if (cs != cudaStreamCaptureStatusNone) {
@@ -797,9 +882,18 @@ int lulesh_job_state_get(lulesh_set *s, int job, lulesh_job_state *out)
     return LULESH_OK;
 }
 
+// the job's origin domain is on another part of a multi-GPU problem
+static bool origin_missing(const lulesh_set *s, int job)
+{
+    if (s->job_origin[job] >= 0) return false;
+    set_error("this part does not hold the subdomain at the mesh origin (rank 0)");
+    return true;
+}
+
 int lulesh_origin_energy(lulesh_set *s, int job, double *energy)
 {
     if (!s || !energy || job < 0 || job >= s->njobs) return LULESH_INVALID_ARG;
+    if (origin_missing(s, job)) return LULESH_INVALID_ARG;
     const DomDev &D = s->hdoms[s->job_origin[job]];
     LCHECK(cudaStreamSynchronize(s->stream));
     LCHECK(cudaMemcpy(energy, D.e + D.octant, sizeof(double), cudaMemcpyDeviceToHost));
@@ -809,6 +903,7 @@ int lulesh_origin_energy(lulesh_set *s, int job, double *energy)
 int lulesh_symmetry(lulesh_set *s, int job, double *max_abs, double *total_abs, double *max_rel)
 {
     if (!s || job < 0 || job >= s->njobs) return LULESH_INVALID_ARG;
+    if (origin_missing(s, job)) return LULESH_INVALID_ARG;
     const DomDev &D = s->hdoms[s->job_origin[job]];
     if (D.unstructured) {
         set_error("the plane-0 symmetry check needs a structured (-s) mesh");

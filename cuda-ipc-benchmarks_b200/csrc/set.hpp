@@ -81,6 +81,24 @@ struct lulesh_set {
     cudaGraphExec_t exec_run = nullptr;
     unsigned long long *run_ctl = nullptr;
 
+    // one part of a problem split over several GPUs (lulesh_create_part):
+    // the local domains hold ranks [first_rank, first_rank + ndom); proxies
+    // of the remote neighbours follow them in the device domain table
+    // (index ndom + k), with their arrays in proxy_arena
+    int nparts = 1, part = 0, first_rank = 0;
+    std::vector<lulesh::DomDev> hproxies;
+    std::vector<int> proxy_rank;
+    void *proxy_arena = nullptr;
+    bool mass_pending = false;  // nodal mass waits for the MASS exchange
+    // pointer tables of the halo pack (send) and unpack (recv) kernels, per
+    // (kind, peer part)
+    struct HaloTable {
+        double **ptrs = nullptr;
+        long long n = 0;
+    };
+    std::vector<int> peers;
+    std::vector<HaloTable> halo_send, halo_recv;  // [kind * peers.size() + peer slot]
+
     // staged comm state: receive-buffer capacity per domain (doubles)
     long com_buf_doubles = 0;
     int max_plane = 0, max_edge = 0;
@@ -120,4 +138,11 @@ void drop_graph(lulesh_set *s);
 int run_status(lulesh_set *s);
 // prepare what enqueue_cycle needs before a capture (staged comm tables)
 int prepare_capture(lulesh_set *s);
+// nodal mass of every subdomain over the whole problem (setup.cu): each node
+// adds volume/8 of the elements touching it in ascending global element
+// index, reading neighbouring subdomains (or their proxies) through nbr
+int nodal_mass_on_device(lulesh_set *s);
+// a part of a multi-GPU problem: the proxies and halo tables (part.cu)
+int part_build(lulesh_set *s);
+void part_release(lulesh_set *s);
 }  // namespace lulesh

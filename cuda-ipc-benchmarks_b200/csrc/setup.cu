@@ -148,7 +148,49 @@ __global__ void k_setup_nodes(DomDev D)
     }
 }
 
+// The init-time nodal mass exchange of a decomposed problem (CommRecv/
+// CommSend/CommSBN of nodalMass, lulesh.cu:4811-4831) as a gather: every
+// node of every subdomain adds volume/8 of the elements touching it over
+// the whole problem, in ascending global element index (the single-domain
+// element loop of lulesh.cu:1165-1187), reading an element of a
+// neighbouring subdomain from that subdomain (or its proxy, whose volo the
+// MASS messages filled).  The sum then equals the single-domain nodal mass
+// bit for bit, where the reference's exchange of partial sums differs in
+// the last bits.  An element outside the mesh has no neighbour (nbr -1).
+__global__ void k_nodal_mass(const DomDev *doms, const int2 *blocks)
+{
+    const int2 blk = blocks[blockIdx.x];
+    const DomDev &D = doms[blk.x];
+    const int n = blk.y + threadIdx.x;
+    if (n >= D.numNode) return;
+    const int nx = D.nx, en = D.en;
+    const int px = n % en, t = n / en, py = t % en, pz = t / en;
+    double m = 0.0;
+    for (int ez = pz - 1; ez <= pz; ++ez)
+        for (int ey = py - 1; ey <= py; ++ey)
+            for (int ex = px - 1; ex <= px; ++ex) {
+                const int sx = ex < 0 ? -1 : (ex >= nx ? 1 : 0);
+                const int sy = ey < 0 ? -1 : (ey >= nx ? 1 : 0);
+                const int sz = ez < 0 ? -1 : (ez >= nx ? 1 : 0);
+                const double *volo = D.volo;
+                if (sx | sy | sz) {
+                    const int nb = D.nbr[(sx + 1) + 3 * (sy + 1) + 9 * (sz + 1)];
+                    if (nb < 0) continue;
+                    volo = doms[nb].volo;
+                }
+                m += volo[((ez - sz * nx) * nx + (ey - sy * nx)) * nx + (ex - sx * nx)] / 8.0;
+            }
+    D.nodalMass[n] = m;
+}
+
 }  // namespace
+
+int nodal_mass_on_device(lulesh_set *s)
+{
+    if (s->n_node_blocks == 0) return LULESH_OK;
+    k_nodal_mass<<<s->n_node_blocks, s->nb, 0, s->stream>>>(s->ddoms, s->node_blocks);
+    return cuda_status(cudaGetLastError(), "nodal mass");
+}
 
 int setup_geometry_on_device(const DomDev &D, double einit, cudaStream_t st)
 {

@@ -1,0 +1,351 @@
+"""One LULESH problem over several GPUs: the reference's multi-rank run.
+
+The reference runs one MPI rank per GPU, each with one subdomain of a cube
+decomposition (InitMeshDecomp, LULESH/cuda/src/lulesh.cu:4606-4668), and
+moves halos between ranks three times per cycle (CommSBN of the nodal
+forces, CommSyncPosVel, CommMonoQ; lulesh.cu:2897-2921, 3061-3094,
+4165-4190) plus one MIN reduction of dt (lulesh.cu:1423-1429), through one
+of its comm backends (LULESH/cuda/README.md:18-113).
+
+Here each process drives one GPU's *part*: a set of consecutive subdomains
+(lulesh_create_part) plus proxies of the neighbours that live on other
+parts.  What crosses between parts is planned by lulesh_halo_plan: corner
+forces instead of partial nodal sums, so every node still adds its corners
+in corner order over the whole mesh and a decomposed run gives the
+single-domain results bit for bit (the in-device 2x2x2 run does the same).
+
+Pieces:
+  GpuPart          one GPU's part: the set, its device message buffers, and
+                   the phase / pack / unpack / dt calls of the C ABI
+  NcclTransport    torch.distributed over NCCL: grouped send/recv of the
+                   device buffers, all_reduce(MIN) of the dt record; one
+                   part per process
+  HostTransport    the same over a host backend (gloo): device -> host,
+                   send/recv and all_reduce on the host, host -> device
+  LocalTransport   every part in this process (device copies); lets one GPU
+                   run the whole multi-part path
+  Engine           the cycle: phases, the three exchanges, the dt reduction
+
+A rank that fails or never arrives makes the others' next exchange end with
+an error after the process group's timeout (no device-side waiting is
+involved: the transports block on the host).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+import lulesh_b200 as L
+
+KINDS = (L.HALO_CORNERS, L.HALO_POSVEL, L.HALO_MONOQ, L.HALO_MASS)
+CYCLE_KINDS = (L.HALO_CORNERS, L.HALO_POSVEL, L.HALO_MONOQ)
+
+
+# ---------------------------------------------------------------------------
+# the plan (host only)
+
+def part_of(rank: int, tp: int, nparts: int) -> int:
+    """Part holding subdomain `rank` (rank * nparts // tp^3)."""
+    return int(L.load_library().lulesh_part_of(rank, tp, nparts))
+
+
+def peers(tp: int, nparts: int, part: int) -> list[int]:
+    lib = L.load_library()
+    buf = (ctypes.c_int * 64)()
+    n = lib.lulesh_halo_peers(tp, nparts, part, buf, 64)
+    if n < 0:
+        raise ValueError(f"lulesh_halo_peers({tp}, {nparts}, {part}) = {n}")
+    return [buf[i] for i in range(n)]
+
+
+def plan(nx: int, tp: int, nparts: int, src: int, dst: int, kind: int):
+    """The message of `kind` from part src to part dst: arrays (rank, field
+    id, index), item i being field[i] of subdomain rank[i] at index[i]."""
+    lib = L.load_library()
+    n = lib.lulesh_halo_plan(nx, tp, nparts, src, dst, kind, None, None, None, 0)
+    if n < 0:
+        raise ValueError(f"lulesh_halo_plan: status {n}")
+    r = np.empty(n, np.int32)
+    f = np.empty(n, np.int32)
+    i = np.empty(n, np.int64)
+    lib.lulesh_halo_plan(nx, tp, nparts, src, dst, kind,
+                         r.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                         f.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                         i.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)), n)
+    return r, f, i
+
+
+def weak_scaling_edge(nparts: int, tp: int = 2, elems_per_part: float = 1e6) -> int:
+    """Subdomain edge giving each of nparts GPUs about elems_per_part."""
+    return max(1, int(round((elems_per_part * nparts / tp ** 3) ** (1.0 / 3.0))))
+
+
+# ---------------------------------------------------------------------------
+# one GPU's part
+
+class GpuPart:
+    """The part of a tp^3 problem (subdomains of edge nx) that one GPU holds.
+    All of its work goes to `stream` (default: torch's current stream, which
+    must not be the legacy default stream), the stream torch.distributed
+    orders its NCCL calls after."""
+
+    def __init__(self, nx: int, tp: int, nparts: int, part: int, numReg: int = 11,
+                 balance: int = 1, cost: int = 1, its: int = -1, device: int | None = None,
+                 stream=None):
+        import torch
+
+        self.torch = torch
+        self.lib = L.load_library()
+        self.nx, self.tp, self.nparts, self.part = nx, tp, nparts, part
+        dev = torch.cuda.current_device() if device is None else device
+        h = ctypes.c_void_p()
+        job = L.JobSpec(nx, numReg, balance, cost, its).c()
+        L._check(self.lib, self.lib.lulesh_create_part(ctypes.byref(job), tp, nparts, part, 0,
+                                                       dev, ctypes.byref(h)),
+                 "lulesh_create_part")
+        self.set = L.LuleshSet(_handle=h)
+        self.h = h
+        self.stream = stream if stream is not None else torch.cuda.current_stream(dev)
+        if self.stream.cuda_stream == 0:
+            raise ValueError("GpuPart needs a stream other than the legacy default stream")
+        self.set.set_stream(self.stream.cuda_stream)
+        self.peers = peers(tp, nparts, part)
+        self.send, self.recv = {}, {}
+        for k in KINDS:
+            self.send[k], self.recv[k] = {}, {}
+            for q in self.peers:
+                ns = int(self.lib.lulesh_halo_count(h, k, q, 1))
+                nr = int(self.lib.lulesh_halo_count(h, k, q, 0))
+                if ns < 0 or nr < 0:
+                    raise L.LuleshError(min(ns, nr), "lulesh_halo_count")
+                self.send[k][q] = torch.zeros(ns, dtype=torch.float64, device=dev)
+                self.recv[k][q] = torch.zeros(nr, dtype=torch.float64, device=dev)
+        self.dt = torch.zeros(4, dtype=torch.int64, device=dev)
+
+    def _ck(self, st, what):
+        L._check(self.lib, st, what)
+
+    def phase(self, ph: int) -> None:
+        self._ck(self.lib.lulesh_part_phase(self.h, ph), "lulesh_part_phase")
+
+    def pack(self, kind: int) -> None:
+        for q, b in self.send[kind].items():
+            if b.numel():
+                self._ck(self.lib.lulesh_halo_pack(self.h, kind, q, b.data_ptr()),
+                         "lulesh_halo_pack")
+
+    def unpack(self, kind: int) -> None:
+        for q, b in self.recv[kind].items():
+            if b.numel():
+                self._ck(self.lib.lulesh_halo_unpack(self.h, kind, q, b.data_ptr()),
+                         "lulesh_halo_unpack")
+
+    def dt_pack(self):
+        self._ck(self.lib.lulesh_part_dt_pack(self.h, self.dt.data_ptr()), "lulesh_part_dt_pack")
+        return self.dt
+
+    def dt_unpack(self, buf) -> None:
+        self._ck(self.lib.lulesh_part_dt_unpack(self.h, buf.data_ptr()), "lulesh_part_dt_unpack")
+
+    def finish_setup(self) -> None:
+        self._ck(self.lib.lulesh_part_finish_setup(self.h), "lulesh_part_finish_setup")
+
+    def halo_doubles(self, kinds=CYCLE_KINDS) -> int:
+        """Doubles this part sends per cycle."""
+        return sum(b.numel() for k in kinds for b in self.send[k].values())
+
+    def close(self) -> None:
+        if getattr(self, "set", None) is not None:
+            self.set.close()
+            self.set = None
+
+
+# ---------------------------------------------------------------------------
+# transports
+
+class LocalTransport:
+    """Every part lives in this process: a message is a copy from the
+    sender's buffer into the receiver's (on the current stream)."""
+
+    name = "local"
+
+    def exchange(self, kind, parts) -> None:
+        by_part = {p.part: p for p in parts}
+        for p in parts:
+            for q, buf in p.send[kind].items():
+                if buf.numel():
+                    by_part[q].recv[kind][p.part].copy_(buf)
+
+    def allreduce_min(self, bufs) -> None:
+        m = bufs[0].clone()
+        for b in bufs[1:]:
+            m = m.minimum(b)
+        for b in bufs:
+            b.copy_(m)
+
+
+class NcclTransport:
+    """One part per process; torch.distributed with the NCCL backend
+    (process rank = part).  Grouped send/recv of the device buffers, then
+    all_reduce(MIN) of the dt record, both ordered after the work already
+    on the current stream."""
+
+    name = "nccl"
+
+    def __init__(self, dist):
+        self.dist = dist
+
+    def exchange(self, kind, parts) -> None:
+        (p,) = parts
+        d = self.dist
+        ops = []
+        for q in p.peers:
+            if p.send[kind][q].numel():
+                ops.append(d.P2POp(d.isend, p.send[kind][q], q))
+            if p.recv[kind][q].numel():
+                ops.append(d.P2POp(d.irecv, p.recv[kind][q], q))
+        if ops:
+            for r in d.batch_isend_irecv(ops):
+                r.wait()
+
+    def allreduce_min(self, bufs) -> None:
+        (b,) = bufs
+        self.dist.all_reduce(b, op=self.dist.ReduceOp.MIN)
+
+
+class HostTransport:
+    """One part per process over a host backend (gloo): each message is
+    copied to the host, sent, received, and copied to the device.  Every
+    wait is bounded by timeout_s: a peer that never sends (it failed, or
+    left) ends the exchange with an exception instead of a hang."""
+
+    name = "host"
+
+    def __init__(self, dist, timeout_s: float = 120.0):
+        import datetime
+
+        self.dist = dist
+        self.timeout = datetime.timedelta(seconds=timeout_s)
+
+    def exchange(self, kind, parts) -> None:
+        (p,) = parts
+        d = self.dist
+        reqs, inbox = [], {}
+        for q in p.peers:
+            if p.send[kind][q].numel():
+                reqs.append(d.isend(p.send[kind][q].cpu(), q))
+            if p.recv[kind][q].numel():
+                inbox[q] = p.recv[kind][q].new_empty(p.recv[kind][q].shape, device="cpu")
+                reqs.append(d.irecv(inbox[q], q))
+        for r in reqs:
+            r.wait(self.timeout)
+        for q, t in inbox.items():
+            p.recv[kind][q].copy_(t)
+
+    def allreduce_min(self, bufs) -> None:
+        (b,) = bufs
+        c = b.cpu()
+        self.dist.all_reduce(c, op=self.dist.ReduceOp.MIN)
+        b.copy_(c)
+
+
+# ---------------------------------------------------------------------------
+# the cycle
+
+class Engine:
+    """Drives the parts of this process through set-up and cycles.  The
+    order is that of LagrangeLeapFrog (lulesh.cu:4438-4452) with each halo
+    exchange where the reference calls its comm backend."""
+
+    def __init__(self, parts, transport):
+        self.parts = list(parts)
+        self.transport = transport
+
+    def exchange(self, kind: int) -> None:
+        for p in self.parts:
+            p.pack(kind)
+        self.transport.exchange(kind, self.parts)
+        for p in self.parts:
+            p.unpack(kind)
+
+    def setup(self) -> None:
+        """The init-time nodal mass exchange (lulesh.cu:4811-4831)."""
+        self.exchange(L.HALO_MASS)
+        for p in self.parts:
+            p.finish_setup()
+
+    def _phase(self, *phases) -> None:
+        for p in self.parts:
+            for ph in phases:
+                p.phase(ph)
+
+    def cycle(self) -> None:
+        self._phase(L.PHASE_TIME_INCREMENT, L.PHASE_FORCE)
+        self.exchange(L.HALO_CORNERS)        # CommSend + CommSBN of the forces
+        self._phase(L.PHASE_NODAL)
+        self.exchange(L.HALO_POSVEL)         # CommSyncPosVel
+        self._phase(L.PHASE_POSVEL_SYNC, L.PHASE_KINEMATICS)
+        self.exchange(L.HALO_MONOQ)          # CommMonoQ
+        self._phase(L.PHASE_MONOQ_GHOST, L.PHASE_EOS)
+        bufs = [p.dt_pack() for p in self.parts]
+        self.transport.allreduce_min(bufs)   # MPI_Allreduce(MIN) of dt
+        for p, b in zip(self.parts, bufs):
+            p.dt_unpack(b)
+
+    def run(self, ncycles: int) -> None:
+        for _ in range(ncycles):
+            self.cycle()
+
+    def launches_per_cycle(self) -> int:
+        """Kernels one cycle launches on each part (phases, packs, unpacks,
+        dt pack/unpack; transport kernels not counted)."""
+        p = self.parts[0]
+        n = 7 + 2
+        for k in CYCLE_KINDS:
+            n += sum(1 for b in p.send[k].values() if b.numel())
+            n += sum(1 for b in p.recv[k].values() if b.numel())
+        return n
+
+
+# ---------------------------------------------------------------------------
+# the N-GPU bench leg
+
+def bench_decomposed(warmup: int, steps: int, dist, transport: str = "nccl") -> dict:
+    """Each process (one per GPU) runs its part of a 2x2x2 (or larger cube)
+    decomposition sized so every GPU holds about 1e6 elements; device time
+    of `steps` cycles after `warmup`, max over ranks."""
+    import torch
+
+    world, rank = dist.get_world_size(), dist.get_rank()
+    tp = 2
+    while tp ** 3 < world:
+        tp += 1
+    nx = weak_scaling_edge(world, tp)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    part = GpuPart(nx, tp, world, rank, stream=stream)
+    tr = NcclTransport(dist) if transport == "nccl" else HostTransport(dist)
+    dist.barrier()
+    eng = Engine([part], tr)
+    eng.setup()
+    eng.run(warmup)
+    torch.cuda.synchronize()
+    dist.barrier()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    eng.run(steps)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms = torch.tensor([t0.elapsed_time(t1)], dtype=torch.float64, device="cuda")
+    dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    st = part.set.state()
+    energy = part.set.origin_energy() if part_of(0, tp, world) == rank else None
+    out = {"ms_max_over_ranks": float(ms.item()), "sub_nx": nx, "tp": tp,
+           "global_nx": nx * tp, "zones_total": (nx * tp) ** 3, "transport": tr.name,
+           "energy": energy, "cycle": st["cycle"], "status": st["status"],
+           "launches_per_cycle": eng.launches_per_cycle(),
+           "halo_bytes_per_cycle": 8 * part.halo_doubles()}
+    part.close()
+    return out

@@ -41,7 +41,15 @@ MSG_MONOQ = 3072
 FIELD_IDS = {
     "x": 0, "y": 1, "z": 2, "xd": 3, "yd": 4, "zd": 5, "fx": 6, "fy": 7,
     "fz": 8, "nodalMass": 9, "delv_xi": 10, "delv_eta": 11, "delv_zeta": 12,
+    "fx_elem": 13, "fy_elem": 14, "fz_elem": 15, "volo": 16,
 }
+FIELD_NAMES = {v: k for k, v in FIELD_IDS.items()}
+
+# halo message kinds of a problem split over GPUs (lulesh_halo_plan)
+HALO_CORNERS, HALO_POSVEL, HALO_MONOQ, HALO_MASS = 0, 1, 2, 3
+# phases of a part's cycle (lulesh_part_phase)
+PHASE_TIME_INCREMENT, PHASE_FORCE, PHASE_NODAL, PHASE_POSVEL_SYNC = 0, 1, 2, 3
+PHASE_KINEMATICS, PHASE_MONOQ_GHOST, PHASE_EOS = 4, 5, 6
 
 INT_FIELDS = {
     "nodelist", "lxim", "lxip", "letam", "letap", "lzetam", "lzetap", "elemBC",
@@ -67,7 +75,21 @@ EXPORTED = [
     "lulesh_set_graph_cycles", "lulesh_get_tuning", "lulesh_set_tuning",
     "lulesh_autotune", "lulesh_checkpoint_bytes", "lulesh_checkpoint_save",
     "lulesh_checkpoint_load", "lulesh_run_graph",
+    "lulesh_part_of", "lulesh_halo_peers", "lulesh_halo_plan", "lulesh_create_part",
+    "lulesh_part_finish_setup", "lulesh_halo_count", "lulesh_halo_pack", "lulesh_halo_unpack",
+    "lulesh_part_phase", "lulesh_part_dt_pack", "lulesh_part_dt_unpack", "lulesh_wait_flag",
 ]
+# the host-only planning functions, also exported by liblulesh_host.so
+HOST_PLAN_SIGS = {
+    "lulesh_part_of": (ctypes.c_int, [ctypes.c_int] * 3),
+    "lulesh_halo_peers": (ctypes.c_int, [ctypes.c_int] * 3 + [ctypes.POINTER(ctypes.c_int),
+                                                              ctypes.c_int]),
+    "lulesh_halo_plan": (ctypes.c_longlong,
+                         [ctypes.c_int] * 6 + [ctypes.POINTER(ctypes.c_int),
+                                               ctypes.POINTER(ctypes.c_int),
+                                               ctypes.POINTER(ctypes.c_longlong),
+                                               ctypes.c_longlong]),
+}
 
 
 class ServerConfig(ctypes.Structure):
@@ -184,7 +206,17 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "lulesh_checkpoint_save": (ip, [vp, vp, ctypes.c_size_t]),
         "lulesh_checkpoint_load": (ip, [vp, vp, ctypes.c_size_t]),
         "lulesh_run_graph": (ip, [vp, ctypes.c_longlong]),
+        "lulesh_create_part": (ip, [ctypes.POINTER(Job), ip, ip, ip, ip, ip, ctypes.POINTER(vp)]),
+        "lulesh_part_finish_setup": (ip, [vp]),
+        "lulesh_halo_count": (ctypes.c_longlong, [vp, ip, ip, ip]),
+        "lulesh_halo_pack": (ip, [vp, ip, ip, vp]),
+        "lulesh_halo_unpack": (ip, [vp, ip, ip, vp]),
+        "lulesh_part_phase": (ip, [vp, ip]),
+        "lulesh_part_dt_pack": (ip, [vp, vp]),
+        "lulesh_part_dt_unpack": (ip, [vp, vp]),
+        "lulesh_wait_flag": (ip, [vp, vp, ctypes.c_uint, dp]),
     }
+    sig.update(HOST_PLAN_SIGS)
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
         fn.restype = res

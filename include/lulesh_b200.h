@@ -353,7 +353,11 @@ double lulesh_server_clock(void);
  * LULESH_NOALLOC_MAX_NX is rejected with LULESH_INVALID_ARG and a message in
  * lulesh_last_error().  The first call on a device looks up that array's
  * device address (with the device current), so make the first call on each
- * device before any stream capture.  All calls share the one array and it
+ * device before any stream capture.  A device reset (cudaDeviceReset) or a
+ * context the caller created itself moves the array, so every call made
+ * outside stream capture looks the address up again; a call on a capturing
+ * stream reuses the address of the last call outside capture, so after a
+ * reset make one call outside capture first.  All calls share the one array and it
  * keeps the last call's contents: calls that overlap on the GPU (different
  * streams, or different host threads, on the same device) race with each
  * other; serialise them on one stream.  Asynchronous on `stream`
@@ -378,7 +382,9 @@ int lulesh_volume_force_noalloc(int nx, const double *x, const double *y, const 
 enum lulesh_field_id {
     LULESH_F_X = 0, LULESH_F_Y, LULESH_F_Z, LULESH_F_XD, LULESH_F_YD,
     LULESH_F_ZD, LULESH_F_FX, LULESH_F_FY, LULESH_F_FZ, LULESH_F_NODALMASS,
-    LULESH_F_DELV_XI, LULESH_F_DELV_ETA, LULESH_F_DELV_ZETA
+    LULESH_F_DELV_XI, LULESH_F_DELV_ETA, LULESH_F_DELV_ZETA,
+    /* moved only by the exchange between GPUs below (not Comm* fields) */
+    LULESH_F_FX_ELEM, LULESH_F_FY_ELEM, LULESH_F_FZ_ELEM, LULESH_F_VOLO
 };
 #define LULESH_MSG_COMM_SBN 1024
 #define LULESH_MSG_SYNC_POS_VEL 2048
@@ -401,6 +407,102 @@ int lulesh_comm_monoq(lulesh_set *set, int rank);
 long lulesh_comm_recv_offset(lulesh_set *set, int recvRank, int dCol,
                              int dRow, int dPlane, int xferFields, int doRecv,
                              int planeOnly);
+
+/* ---- one problem over several GPUs ------------------------------------ */
+/* The reference's multi-rank run (one rank per GPU, halos over MPI / CUDA
+ * IPC / NVSHMEM: LULESH/cuda/README.md:18-113, lulesh-comms-direct.cu:
+ * 50-404, comm/comm_ipc_common.h:26-261) as parts: the tp^3 subdomains of
+ * one problem are split over `nparts` GPUs, one process (and one set) per
+ * GPU; rank r belongs to part lulesh_part_of(r, tp, nparts) = r * nparts /
+ * tp^3.  A subdomain whose neighbour sits on another part reads that
+ * neighbour through a proxy: arrays in the neighbour's layout whose boundary
+ * layers the messages below fill.  The cycle's kernels are those of an
+ * in-device subdomain set, so a decomposed run gives the single-domain
+ * results bit for bit, like the in-device 2x2x2 run.
+ *
+ * Messages (kind, from part, to part) are planned by lulesh_halo_plan: item
+ * i is field[i] of subdomain rank[i] at index[i], and lands at the same
+ * index of the receiver's proxy of that subdomain.  Kinds:
+ *   CORNERS  corner forces of the element layers facing the receiver
+ *            (replaces CommSend/CommSBN of fx/fy/fz, lulesh.cu:2897-2921:
+ *            the receiver adds every node's corners in corner order, so no
+ *            partial sums and no float atomics cross)
+ *   POSVEL   x..zd of the node layers facing a receiver on the minus sides
+ *            (CommSyncPosVel, lulesh.cu:3061-3094)
+ *   MONOQ    delv_xi/eta/zeta of the element face layers (CommMonoQ,
+ *            lulesh.cu:4165-4190)
+ *   MASS     volo of the element layers, once at set-up (the init-time
+ *            nodalMass CommSBN, lulesh.cu:4811-4831)
+ * The host functions (lulesh_part_of, lulesh_halo_peers, lulesh_halo_plan)
+ * need no GPU. */
+#define LULESH_HALO_CORNERS 0
+#define LULESH_HALO_POSVEL 1
+#define LULESH_HALO_MONOQ 2
+#define LULESH_HALO_MASS 3
+
+int lulesh_part_of(int rank, int tp, int nparts);
+/* The parts that `part` exchanges messages with, ascending, into peers[]
+ * (up to max_peers); returns their number or a negative status. */
+int lulesh_halo_peers(int tp, int nparts, int part, int *peers, int max_peers);
+/* Plan of one message; returns the number of items (the message length in
+ * doubles) and fills up to max_items of rank/field/index (each may be
+ * NULL), or a negative status. */
+long long lulesh_halo_plan(int nx, int tp, int nparts, int from_part, int to_part, int kind,
+                           int *rank, int *field, long long *index, long long max_items);
+
+/* This GPU's part of the problem: the subdomains it owns (domains
+ * 0..n-1 of the set in rank order) and proxies of their neighbours on other
+ * parts.  Before the first cycle, exchange the MASS messages with every
+ * peer (pack, move, unpack) and call lulesh_part_finish_setup, which sums
+ * each node's mass over the elements of the whole problem that touch it,
+ * on the device.  nparts = 1 gives an ordinary subdomain set.  FP64 and
+ * the fused exchange only (no LULESH_FLAG_MIXED / LULESH_FLAG_COMM_STAGED);
+ * a part of several GPUs advances through lulesh_part_phase, not
+ * lulesh_step. */
+int lulesh_create_part(const lulesh_job *job, int tp, int nparts, int part, int flags,
+                       int device, lulesh_set **out);
+int lulesh_part_finish_setup(lulesh_set *set);
+
+/* Length in doubles of the message of `kind` this part sends to
+ * (to_peer = 1) or receives from (to_peer = 0) part `peer`. */
+long long lulesh_halo_count(lulesh_set *set, int kind, int peer, int to_peer);
+/* Enqueue on the set's stream: gather the message for `peer` into dev_buf,
+ * or scatter the message received from `peer` into the proxies.  dev_buf
+ * is caller-owned device memory of lulesh_halo_count doubles. */
+int lulesh_halo_pack(lulesh_set *set, int kind, int peer, double *dev_buf);
+int lulesh_halo_unpack(lulesh_set *set, int kind, int peer, const double *dev_buf);
+
+/* One phase of the cycle, enqueued on the set's stream.  A cycle of a part
+ * is: TIME_INCREMENT, FORCE, exchange CORNERS, NODAL, exchange POSVEL,
+ * POSVEL_SYNC, KINEMATICS, exchange MONOQ, MONOQ_GHOST, EOS, then the dt
+ * reduction below. */
+#define LULESH_PHASE_TIME_INCREMENT 0
+#define LULESH_PHASE_FORCE 1
+#define LULESH_PHASE_NODAL 2
+#define LULESH_PHASE_POSVEL_SYNC 3
+#define LULESH_PHASE_KINEMATICS 4
+#define LULESH_PHASE_MONOQ_GHOST 5
+#define LULESH_PHASE_EOS 6
+int lulesh_part_phase(lulesh_set *set, int phase);
+
+/* The dt reduction of TimeIncrement (MPI_Allreduce MIN, lulesh.cu:
+ * 1423-1429) and the error flags of checkErrors: dt_pack writes this
+ * part's four int64 values (courant and hydro dt minima as IEEE bit
+ * patterns, the smallest element with a volume error and with q above
+ * qstop, INT_MAX for none) to dev_buf; the caller takes the element-wise
+ * minimum over all parts (e.g. ncclAllReduce MIN on int64) and hands the
+ * result to dt_unpack before the next TIME_INCREMENT. */
+int lulesh_part_dt_pack(lulesh_set *set, long long *dev_buf);
+int lulesh_part_dt_unpack(lulesh_set *set, const long long *dev_buf);
+
+/* Bounded wait on a device flag for transports that signal arrival with a
+ * flag the sender sets in this GPU's memory (peer stores): enqueues a
+ * one-thread kernel that spins until *flag >= expect or timeout_ms has
+ * passed; on timeout the set's job is stopped with status LULESH_TIMEOUT
+ * (read by lulesh_job_state_get) and the kernel returns, so the context
+ * stays usable. */
+int lulesh_wait_flag(lulesh_set *set, const unsigned int *dev_flag, unsigned int expect,
+                     double timeout_ms);
 
 #ifdef __cplusplus
 }

@@ -81,6 +81,12 @@ struct OracleDomain {
     int bad_vol, bad_q;
     /* element holding the energy deposit (0 on -s meshes) */
     int octantCorner;
+    /* decomposed stepping: ghost-face offsets into delv_* (SetupConnectivityBC
+     * order, INT_MIN for none) and the 26 neighbours' arrays, by direction
+     * (dx+1) + 3(dy+1) + 9(dz+1) */
+    int ghost[6];
+    OracleMirror mirror[27];
+    int has_mirror[27];
 };
 
 static void *zalloc(size_t n) { return calloc(n ? n : 1, 1); }
@@ -681,6 +687,7 @@ OracleDomain *oracle_create(int nx, int numReg, int balance, int cost,
     if (d->rowMax) { ghost[3] = pidx; pidx += nx * nx; }
     if (d->colMin) { ghost[4] = pidx; pidx += nx * nx; }
     if (d->colMax) { ghost[5] = pidx; }
+    for (int i = 0; i < 6; ++i) d->ghost[i] = ghost[i];
     for (int i = 0; i < nx; ++i) {
         int planeInc = i * nx * nx, rowInc = i * nx;
         for (int j = 0; j < nx; ++j) {
@@ -1416,6 +1423,218 @@ int oracle_run(OracleDomain *d, int its, int *cycles_run)
     }
     if (cycles_run) *cycles_run = n;
     return st;
+}
+
+/* ------------------------------------------------------------------ */
+/* decomposed stepping                                                  */
+/* ------------------------------------------------------------------ */
+
+void oracle_set_mirror(OracleDomain *d, int dir, const OracleMirror *m)
+{
+    if (dir < 0 || dir >= 27) return;
+    d->has_mirror[dir] = m != NULL;
+    if (m) d->mirror[dir] = *m;
+}
+
+/* corner forces (the first loop of volume_force) */
+static void corner_forces(OracleDomain *d)
+{
+    const int Ep = d->Ep;
+    const double hourg = d->hgcoef;
+    for (int el = 0; el < d->numElem; ++el) {
+        double xn[8], yn[8], zn[8], xdn[8], ydn[8], zdn[8];
+        double dvdx[8], dvdy[8], dvdz[8], hgfx[8], hgfy[8], hgfz[8];
+        double hg[8][4], B[3][8];
+        double volume = d->v[el];
+        double det = d->volo[el] * volume;
+        if (volume < 0.) d->bad_vol = el;
+        double ss1 = d->ss[el], mass1 = d->elemMass[el];
+        double sigxx = -d->p[el] - d->q[el];
+        int n[8];
+        for (int k = 0; k < 8; ++k) n[k] = d->nodelist[el + k * Ep];
+        double volinv = 1.0 / det;
+        for (int k = 0; k < 8; ++k) {
+            xn[k] = d->x[n[k]];
+            yn[k] = d->y[n[k]];
+            zn[k] = d->z[n[k]];
+        }
+        double volume13 = cbrt(det);
+        double coefficient = -hourg * 0.01 * ss1 * mass1 / volume13;
+        volume_derivative(dvdx, dvdy, dvdz, xn, yn, zn);
+        hourglass_modes(xn, yn, zn, dvdx, dvdy, dvdz, hg, volinv);
+        shape_derivs(xn, yn, zn, B, &det);
+        node_normals(B[0], B[1], B[2], xn, yn, zn);
+        if (det < 0.) d->bad_vol = el;
+        for (int k = 0; k < 8; ++k) {
+            hgfx[k] = -(sigxx * B[0][k]);
+            hgfy[k] = -(sigxx * B[1][k]);
+            hgfz[k] = -(sigxx * B[2][k]);
+        }
+        if (hourg > 0.0) {
+            for (int k = 0; k < 8; ++k) {
+                xdn[k] = d->xd[n[k]];
+                ydn[k] = d->yd[n[k]];
+                zdn[k] = d->zd[n[k]];
+            }
+            fb_hourglass(xdn, hg, coefficient, hgfx);
+            fb_hourglass(ydn, hg, coefficient, hgfy);
+            fb_hourglass(zdn, hg, coefficient, hgfz);
+        }
+        for (int k = 0; k < 8; ++k) {
+            d->fx_elem[el + Ep * k] = hgfx[k];
+            d->fy_elem[el + Ep * k] = hgfy[k];
+            d->fz_elem[el + Ep * k] = hgfz[k];
+        }
+    }
+}
+
+static const int kCX[8] = {0, 1, 1, 0, 0, 1, 1, 0};
+static const int kCY[8] = {0, 0, 1, 1, 0, 0, 1, 1};
+static const int kCZ[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+
+static int axis_side(int v, int n) { return v < 0 ? -1 : (v >= n ? 1 : 0); }
+static int dir_index(int sx, int sy, int sz) { return (sx + 1) + 3 * (sy + 1) + 9 * (sz + 1); }
+
+/* Node force sums over the whole problem: every node of the subdomain adds
+ * the corner forces of the elements that touch it in corner order j = 0..7
+ * (the order of nodeElemCornerList on the undecomposed mesh,
+ * lulesh.cu:1079-1088), taking an element of a neighbouring subdomain from
+ * that neighbour's mirror; then the node update. */
+static void nodal_decomposed(OracleDomain *d)
+{
+    const int nx = d->nx, en = nx + 1;
+    for (int i = 0; i < d->numNode; ++i) {
+        const int px = i % en, py = (i / en) % en, pz = i / (en * en);
+        double fx = 0.0, fy = 0.0, fz = 0.0;
+        for (int j = 0; j < 8; ++j) {
+            const int ex = px - kCX[j], ey = py - kCY[j], ez = pz - kCZ[j];
+            const int sx = axis_side(ex, nx), sy = axis_side(ey, nx), sz = axis_side(ez, nx);
+            const int c = j * d->Ep + ((ez - sz * nx) * nx + (ey - sy * nx)) * nx + (ex - sx * nx);
+            if ((sx | sy | sz) == 0) {
+                fx += d->fx_elem[c];
+                fy += d->fy_elem[c];
+                fz += d->fz_elem[c];
+            } else {
+                const int k = dir_index(sx, sy, sz);
+                if (!d->has_mirror[k]) continue;
+                fx += d->mirror[k].fx_elem[c];
+                fy += d->mirror[k].fy_elem[c];
+                fz += d->mirror[k].fz_elem[c];
+            }
+        }
+        d->fx[i] = fx;
+        d->fy[i] = fy;
+        d->fz[i] = fz;
+    }
+    nodal_update(d);
+}
+
+/* CommSyncPosVel: a node on a max face shared with a neighbour takes
+ * x..zd from the neighbour that holds it on its min faces */
+static void posvel_decomposed(OracleDomain *d)
+{
+    const int nx = d->nx, en = nx + 1, tp = d->tp;
+    for (int i = 0; i < d->numNode; ++i) {
+        const int px = i % en, py = (i / en) % en, pz = i / (en * en);
+        const int sx = (px == nx && d->colLoc < tp - 1);
+        const int sy = (py == nx && d->rowLoc < tp - 1);
+        const int sz = (pz == nx && d->planeLoc < tp - 1);
+        if ((sx | sy | sz) == 0) continue;
+        const int k = dir_index(sx, sy, sz);
+        if (!d->has_mirror[k]) continue;
+        const OracleMirror *m = &d->mirror[k];
+        const int j = ((pz - sz * nx) * en + (py - sy * nx)) * en + (px - sx * nx);
+        d->x[i] = m->x[j];
+        d->y[i] = m->y[j];
+        d->z[i] = m->z[j];
+        d->xd[i] = m->xd[j];
+        d->yd[i] = m->yd[j];
+        d->zd[i] = m->zd[j];
+    }
+}
+
+/* CommMonoQ: the delv_* ghost faces take the neighbour's boundary layer */
+static void monoq_ghosts_decomposed(OracleDomain *d)
+{
+    const int nx = d->nx;
+    static const int dirs[6][3] = {{0, 0, -1}, {0, 0, 1}, {0, -1, 0},
+                                   {0, 1, 0},  {-1, 0, 0}, {1, 0, 0}};
+    for (int f = 0; f < 6; ++f) {
+        if (d->ghost[f] == INT_MIN) continue;
+        const int k = dir_index(dirs[f][0], dirs[f][1], dirs[f][2]);
+        if (!d->has_mirror[k]) continue;
+        const OracleMirror *m = &d->mirror[k];
+        for (int a = 0; a < nx; ++a)
+            for (int b = 0; b < nx; ++b) {
+                int src;
+                switch (f) {
+                    case 0: src = ((nx - 1) * nx + a) * nx + b; break;
+                    case 1: src = (0 * nx + a) * nx + b; break;
+                    case 2: src = (a * nx + (nx - 1)) * nx + b; break;
+                    case 3: src = (a * nx + 0) * nx + b; break;
+                    case 4: src = (a * nx + b) * nx + (nx - 1); break;
+                    default: src = (a * nx + b) * nx + 0; break;
+                }
+                const int g = d->ghost[f] + a * nx + b;
+                d->delv_xi[g] = m->delv_xi[src];
+                d->delv_eta[g] = m->delv_eta[src];
+                d->delv_zeta[g] = m->delv_zeta[src];
+            }
+    }
+}
+
+int oracle_phase(OracleDomain *d, int phase)
+{
+    switch (phase) {
+        case ORACLE_PHASE_TIME_INCREMENT: time_increment(d); break;
+        case ORACLE_PHASE_FORCE: corner_forces(d); break;
+        case ORACLE_PHASE_NODAL: nodal_decomposed(d); break;
+        case ORACLE_PHASE_POSVEL_SYNC: posvel_decomposed(d); break;
+        case ORACLE_PHASE_KINEMATICS: kinematics(d); break;
+        case ORACLE_PHASE_MONOQ_GHOST: monoq_ghosts_decomposed(d); break;
+        case ORACLE_PHASE_EOS:
+            monoq_region(d);
+            eos(d);
+            time_constraints(d);
+            break;
+        default: return -5;
+    }
+    if (d->bad_vol != -1) return -1;
+    if (d->bad_q != -1) return -2;
+    return 0;
+}
+
+/* nodalMass over the whole problem: the volume/8 of every element that
+ * touches the node, in ascending global element index (the single-domain
+ * element loop of lulesh.cu:1165-1187), neighbours' volumes from mirrors */
+void oracle_nodal_mass_decomposed(OracleDomain *d)
+{
+    const int nx = d->nx, en = nx + 1;
+    for (int i = 0; i < d->numNode; ++i) {
+        const int px = i % en, py = (i / en) % en, pz = i / (en * en);
+        double m = 0.0;
+        for (int ez = pz - 1; ez <= pz; ++ez)
+            for (int ey = py - 1; ey <= py; ++ey)
+                for (int ex = px - 1; ex <= px; ++ex) {
+                    const int sx = axis_side(ex, nx), sy = axis_side(ey, nx),
+                              sz = axis_side(ez, nx);
+                    const int e = ((ez - sz * nx) * nx + (ey - sy * nx)) * nx + (ex - sx * nx);
+                    if ((sx | sy | sz) == 0) {
+                        m += d->volo[e] / 8.0;
+                    } else {
+                        const int k = dir_index(sx, sy, sz);
+                        if (!d->has_mirror[k]) continue;  /* outside the mesh */
+                        m += d->mirror[k].volo[e] / 8.0;
+                    }
+                }
+        d->nodalMass[i] = m;
+    }
+}
+
+void oracle_set_dt_minima(OracleDomain *d, double dtcourant, double dthydro)
+{
+    d->dtcourant = dtcourant;
+    d->dthydro = dthydro;
 }
 
 /* ------------------------------------------------------------------ */

@@ -57,6 +57,38 @@ int *oracle_int_field(OracleDomain *d, const char *name, int *count);
 double oracle_scalar(OracleDomain *d, const char *name);
 void oracle_set_deltatime(OracleDomain *d, double dt);
 
+/* ---- decomposed stepping -------------------------------------------- */
+/* One subdomain of a tp^3 problem stepped phase by phase, reading its
+ * neighbours through mirrors: arrays in each neighbour's own layout (the
+ * neighbour's real arrays, or copies of whatever parts a halo exchange has
+ * filled).  Used to check an exchange between processes on the CPU: with
+ * every mirror holding what the neighbour holds, a decomposed run gives the
+ * single-domain values bit for bit (node sums in corner order over the
+ * whole mesh, nodal mass in ascending global element order). */
+typedef struct OracleMirror {
+    const double *x, *y, *z, *xd, *yd, *zd;
+    const double *fx_elem, *fy_elem, *fz_elem;
+    const double *delv_xi, *delv_eta, *delv_zeta;
+    const double *volo;
+} OracleMirror;
+
+#define ORACLE_PHASE_TIME_INCREMENT 0
+#define ORACLE_PHASE_FORCE 1       /* corner forces only */
+#define ORACLE_PHASE_NODAL 2       /* node sums (mirrors) + node update */
+#define ORACLE_PHASE_POSVEL_SYNC 3 /* x..zd from the +side owner */
+#define ORACLE_PHASE_KINEMATICS 4
+#define ORACLE_PHASE_MONOQ_GHOST 5 /* delv_* ghost faces from mirrors */
+#define ORACLE_PHASE_EOS 6         /* monoQ region, EOS, dt constraints */
+
+/* dir = (dx+1) + 3(dy+1) + 9(dz+1); m NULL clears (the copy of the struct
+ * is kept; the arrays must outlive the stepping) */
+void oracle_set_mirror(OracleDomain *d, int dir, const OracleMirror *m);
+int oracle_phase(OracleDomain *d, int phase);
+void oracle_nodal_mass_decomposed(OracleDomain *d);
+/* the dt minima the next TIME_INCREMENT uses (after a reduction over
+ * subdomains) */
+void oracle_set_dt_minima(OracleDomain *d, double dtcourant, double dthydro);
+
 /* VerifyAndWriteFinalOutput numbers (lulesh.cu:4700-4736). */
 double oracle_origin_energy(OracleDomain *d);
 void oracle_symmetry(OracleDomain *d, double *max_abs, double *total_abs,

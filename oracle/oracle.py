@@ -27,6 +27,14 @@ INT_FIELDS = {
 
 _lib = None
 
+MIRROR_FIELDS = ("x", "y", "z", "xd", "yd", "zd", "fx_elem", "fy_elem", "fz_elem",
+                 "delv_xi", "delv_eta", "delv_zeta", "volo")
+
+
+class OracleMirror(ctypes.Structure):
+    """A neighbour's arrays for decomposed stepping (lulesh_oracle.h)."""
+    _fields_ = [(f, ctypes.POINTER(ctypes.c_double)) for f in MIRROR_FIELDS]
+
 
 def build() -> None:
     subprocess.run(["make", "-C", HERE, "liboracle.so"], check=True,
@@ -60,6 +68,11 @@ def load() -> ctypes.CDLL:
     lib.oracle_origin_energy.restype = dp
     lib.oracle_origin_energy.argtypes = [vp]
     lib.oracle_symmetry.argtypes = [vp] + [ctypes.POINTER(dp)] * 3
+    lib.oracle_set_mirror.argtypes = [vp, ip, ctypes.POINTER(OracleMirror)]
+    lib.oracle_phase.restype = ip
+    lib.oracle_phase.argtypes = [vp, ip]
+    lib.oracle_nodal_mass_decomposed.argtypes = [vp]
+    lib.oracle_set_dt_minima.argtypes = [vp, dp, dp]
     _lib = lib
     return lib
 
@@ -123,6 +136,37 @@ class Oracle:
         p = self.lib.oracle_real_field(self.h, name.encode(), ctypes.byref(n))
         arr = np.ctypeslib.as_array(p, shape=(n.value,))
         arr[:] = values
+
+    def view(self, name: str) -> np.ndarray:
+        """The oracle's own array (no copy): writes go into the domain."""
+        n = ctypes.c_int()
+        p = self.lib.oracle_real_field(self.h, name.encode(), ctypes.byref(n))
+        if not p:
+            raise KeyError(name)
+        return np.ctypeslib.as_array(p, shape=(n.value,))
+
+    # -- decomposed stepping (a subdomain whose neighbours are read through
+    #    mirrors; lulesh_oracle.h)
+    def set_mirror(self, direction: int, arrays: dict | None) -> None:
+        """arrays: name -> float64 numpy array (kept alive by the caller)."""
+        if arrays is None:
+            self.lib.oracle_set_mirror(self.h, direction, None)
+            return
+        m = OracleMirror(*[arrays[f].ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+                           for f in MIRROR_FIELDS])
+        self.lib.oracle_set_mirror(self.h, direction, ctypes.byref(m))
+
+    def phase(self, ph: int) -> int:
+        return self.lib.oracle_phase(self.h, ph)
+
+    def nodal_mass_decomposed(self) -> None:
+        self.lib.oracle_nodal_mass_decomposed(self.h)
+
+    def set_dt_minima(self, dtcourant: float, dthydro: float) -> None:
+        self.lib.oracle_set_dt_minima(self.h, dtcourant, dthydro)
+
+    def set_deltatime(self, dt: float) -> None:
+        self.lib.oracle_set_deltatime(self.h, dt)
 
     def scalar(self, name: str) -> float:
         return self.lib.oracle_scalar(self.h, name.encode())

@@ -4,7 +4,7 @@ LULESH/cuda/src by oracle/Makefile for sm_100a with the 17-digit print hook).
 It needs a B200, so it runs on a GPU machine with the built tree:
 
     make -C oracle ref                         # in the build container
-    python tests/golden/make_golden_cuda.py    # on the GPU machine
+    python tests/golden/make_golden_cuda.py [out.json]   # on the GPU machine
 
 The reference CUDA command line is `lulesh -s N x ITERS` (lulesh.cu:4754-4770;
 argv[4] is the iteration cap, -1 runs to the stop time); it fixes
@@ -30,6 +30,13 @@ CASES = [
     (90, 200),     # the published -s 45 x 8 ranks case as one domain
     (100, 500),    # config 2
     (120, 1000),   # config 4 FP64 reference
+    # -s 100 after the cycle counts bench.py ends its timed region on
+    # (warm-up + steps: 5 + 20, 5 + 100, 5 + 500, 5 + 1000); the bench checks
+    # its energy against these
+    (100, 25),
+    (100, 105),
+    (100, 505),
+    (100, 1005),
 ]
 
 
@@ -50,7 +57,10 @@ def main():
                   "print hook",
         "runs": runs,
     }
-    with open(os.path.join(HERE, "cuda_reference.json"), "w") as f:
+    # an optional path argument writes the table elsewhere (to bring it back
+    # from the GPU machine); the default is the committed fixture
+    out = sys.argv[1] if len(sys.argv) > 1 else os.path.join(HERE, "cuda_reference.json")
+    with open(out, "w") as f:
         json.dump(doc, f, indent=1)
 
 

@@ -20,7 +20,13 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-RTOL = 1e-12  # the parity tolerance of the one-cycle field tests
+# The no-allocation kernel evaluates every force expression in the same
+# written form, and sums each node's corners in the same order (corner 0..7),
+# as the regular force and nodal kernels, so nvcc makes the same multiply-add
+# contractions and the forces agree bit for bit; RTOL is the parity tolerance
+# of the one-cycle field tests, kept as the bound the bit-for-bit check
+# tightens.
+RTOL = 1e-12
 
 NODE_IN = ["x", "y", "z", "xd", "yd", "zd"]
 ELEM_IN = ["volo", "v", "p", "q", "ss", "elemMass"]
@@ -44,10 +50,10 @@ def _state(s):
     return {k: s.field(k) for k in NODE_IN + ELEM_IN}
 
 
-def test_noalloc_forces_match_regular_entry_point(lulesh):
+@pytest.mark.parametrize("nx", [14, 32])  # 32: the array's full capacity (32,768 elements)
+def test_noalloc_forces_match_regular_entry_point(lulesh, nx):
     torch = pytest.importorskip("torch")
     lib = lulesh.load_library()
-    nx = 14
     with lulesh.LuleshSet(nx=nx, its=-1, flags=lulesh.FLAG_MATERIALIZE, device=0) as s:
         # at cycle 0 pressure and velocity are zero everywhere and so is every
         # force; a few cycles in, the blast gives both calls non-zero forces
@@ -62,6 +68,7 @@ def test_noalloc_forces_match_regular_entry_point(lulesh):
             for g, r in zip(got, ref):
                 scale = max(float(np.max(np.abs(r))), 1e-300)
                 assert np.allclose(g, r, rtol=RTOL, atol=RTOL * scale), f"call {call}"
+                assert np.array_equal(g, r), f"call {call}: not bit-identical"
             assert np.any(got[0] != 0.0)
 
 
@@ -82,3 +89,72 @@ def test_noalloc_reports_volume_error(lulesh):
     state["v"][7] = -1.0
     st, _, bad = _call(lib, torch, nx, state)
     assert st == lulesh.OK and bad == 7
+
+
+_RESET_CHILD = r"""
+import ctypes, sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+import lulesh_b200 as L
+
+lib = L.load_library()
+rt = ctypes.CDLL("libcudart.so.12")  # the runtime the library already loaded
+NODE_IN = ["x", "y", "z", "xd", "yd", "zd"]
+ELEM_IN = ["volo", "v", "p", "q", "ss", "elemMass"]
+nx = 8
+with L.LuleshSet(nx=nx, its=-1, device=0) as s:
+    s.step(4)
+    state = [s.field(k) for k in NODE_IN + ELEM_IN]
+
+def ck(e, what):
+    if e != 0:
+        raise SystemExit(f"{what}: cudaError {e}")
+
+def forces():
+    ptrs = []
+    for a in state:
+        p = ctypes.c_void_p()
+        ck(rt.cudaMalloc(ctypes.byref(p), ctypes.c_size_t(a.nbytes)), "cudaMalloc")
+        ck(rt.cudaMemcpy(p, a.ctypes.data_as(ctypes.c_void_p), ctypes.c_size_t(a.nbytes), 1),
+           "cudaMemcpy H2D")
+        ptrs.append(p)
+    nn = (nx + 1) ** 3
+    outs = []
+    for _ in range(3):
+        p = ctypes.c_void_p()
+        ck(rt.cudaMalloc(ctypes.byref(p), ctypes.c_size_t(8 * nn)), "cudaMalloc")
+        outs.append(p)
+    st = lib.lulesh_volume_force_noalloc(nx, *ptrs, 3.0, *outs, None, None)
+    if st != 0:
+        raise SystemExit(f"noalloc status {st}: {lib.lulesh_last_error()}")
+    ck(rt.cudaDeviceSynchronize(), "cudaDeviceSynchronize")
+    res = []
+    for p in outs:
+        h = np.empty(nn, dtype=np.float64)
+        ck(rt.cudaMemcpy(h.ctypes.data_as(ctypes.c_void_p), p, ctypes.c_size_t(8 * nn), 2),
+           "cudaMemcpy D2H")
+        res.append(h)
+    for p in ptrs + outs:
+        ck(rt.cudaFree(p), "cudaFree")
+    return res
+
+before = forces()
+ck(rt.cudaDeviceReset(), "cudaDeviceReset")  # ends this process's own context only
+after = forces()
+assert all(np.array_equal(a, b) for a, b in zip(before, after)), "forces changed"
+assert np.any(before[0] != 0.0)
+print("RESET_OK")
+"""
+
+
+def test_noalloc_after_device_reset(lulesh):
+    """A device reset reloads the library's module, which may move the
+    scratch array; the next call looks its address up again and gives the
+    same forces.  Run in a child process so the reset ends only that
+    process's own context, not the one the other tests share."""
+    import subprocess
+    import sys
+
+    r = subprocess.run([sys.executable, "-c", _RESET_CHILD, lulesh.HERE],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "RESET_OK" in r.stdout, r.stdout + r.stderr
