@@ -15,13 +15,15 @@ namespace lulesh {
 namespace {
 
 constexpr unsigned kMagic = 0x4c554c43u;  // "LULC"
-constexpr unsigned kVersion = 1;
+constexpr unsigned kVersion = 2;
 
 struct CkptHeader {
     unsigned magic, version;
     int njobs, ndom, tp, flags;
     unsigned long long arena_bytes, tc_bytes;
     unsigned long long jobs_hash;  // FNV-1a of the job descriptions
+    unsigned long long mesh_hash;  // an lmesh set's mesh (lulesh_set::mesh_hash)
+    int nparts, part;              // a part of a problem split over GPUs
 };
 
 unsigned long long jobs_hash(const lulesh_set *s)
@@ -47,6 +49,9 @@ CkptHeader header_of(const lulesh_set *s)
     h.arena_bytes = s->arena_bytes;
     h.tc_bytes = sizeof(TimeCtl) * s->njobs;
     h.jobs_hash = jobs_hash(s);
+    h.mesh_hash = s->mesh_hash;
+    h.nparts = s->nparts;
+    h.part = s->part;
     return h;
 }
 
@@ -101,8 +106,10 @@ int lulesh_checkpoint_load(lulesh_set *s, const void *buf, size_t bytes)
     }
     if (h.njobs != mine.njobs || h.ndom != mine.ndom || h.tp != mine.tp ||
         h.flags != mine.flags || h.arena_bytes != mine.arena_bytes ||
-        h.tc_bytes != mine.tc_bytes || h.jobs_hash != mine.jobs_hash) {
-        set_error("lulesh_checkpoint_load: checkpoint of a different set (jobs, tp or flags)");
+        h.tc_bytes != mine.tc_bytes || h.jobs_hash != mine.jobs_hash ||
+        h.mesh_hash != mine.mesh_hash || h.nparts != mine.nparts || h.part != mine.part) {
+        set_error("lulesh_checkpoint_load: checkpoint of a different set (jobs, mesh, tp, "
+                  "part or flags)");
         return LULESH_INVALID_ARG;
     }
     if (bytes < lulesh_checkpoint_bytes(s)) {

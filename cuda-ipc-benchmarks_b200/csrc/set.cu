@@ -130,6 +130,18 @@ static int create_common(lulesh_set *s, const std::vector<DomPlace> &place, int 
         }
         commd[0] = 0;
         total = domain_bytes(sizes_of(mesh, 0), mixed);
+        unsigned long long h = 1469598103934665603ull;
+        auto mix = [&h](const void *p, size_t n) {
+            const unsigned char *b = static_cast<const unsigned char *>(p);
+            for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+        };
+        mix(&mesh.numElem, sizeof mesh.numElem);
+        mix(&mesh.numNode, sizeof mesh.numNode);
+        mix(mesh.nodelist.data(), sizeof(int) * mesh.nodelist.size());
+        mix(mesh.x.data(), sizeof(double) * mesh.x.size());
+        mix(mesh.y.data(), sizeof(double) * mesh.y.size());
+        mix(mesh.z.data(), sizeof(double) * mesh.z.size());
+        s->mesh_hash = h;
     } else {
         for (int d = 0; d < s->ndom; ++d) {
             const lulesh_job &j = s->jobs[place[d].job];

@@ -33,6 +33,9 @@ struct lulesh_set {
     // one unstructured domain read from this lmesh file (empty: -s meshes)
     std::string mesh_path;
     bool unstructured = false;
+    // FNV-1a of an unstructured mesh's sizes, connectivity and coordinates
+    // (identifies the mesh in checkpoints; 0 for -s meshes)
+    unsigned long long mesh_hash = 0;
     int ndom = 0, njobs = 0;
 
     // per-domain metadata kept on the host

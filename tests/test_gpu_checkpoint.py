@@ -55,3 +55,23 @@ def test_checkpoint_of_another_set_is_refused(lulesh):
             b.restore(ck[: len(ck) // 2])
         with pytest.raises(lulesh.LuleshError):
             b.restore(b"x" * len(ck))
+
+
+def test_checkpoint_of_another_mesh_file_is_refused(lulesh, tmp_path):
+    """Two lmesh files with the same element and node counts but different
+    geometry: a checkpoint of one loads into a set of the same file and is
+    refused by a set of the other."""
+    import lmesh
+
+    a_path, b_path = tmp_path / "a.lmesh", tmp_path / "b.lmesh"
+    lmesh.write(a_path, lmesh.box(6))
+    lmesh.write(b_path, lmesh.warp(lmesh.box(6)))
+    with lulesh.LuleshSet.from_mesh(str(a_path), its=-1) as a:
+        a.step(3)
+        ck = a.checkpoint()
+    with lulesh.LuleshSet.from_mesh(str(a_path), its=-1) as same:
+        same.restore(ck)
+        assert same.state()["cycle"] == 3
+    with lulesh.LuleshSet.from_mesh(str(b_path), its=-1) as other:
+        with pytest.raises(lulesh.LuleshError):
+            other.restore(ck)

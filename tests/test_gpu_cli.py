@@ -92,3 +92,50 @@ def test_one_launch_gives_the_same_run(tmp_path):
     full = [re.search(r"Origin energy, 17 digits = (\S+)", r.stdout).group(1) for r in outs]
     assert full[0] == full[1]
     assert _awk(outs[0].stdout, "Iteration count", 4) == _awk(outs[1].stdout, "Iteration count", 4)
+
+
+def _read_xyz(path):
+    """xyz.asc as write_solution writes it (lulesh.cu:4584-4603): per node a
+    "%10d" index line, then x, y and z on lines of their own."""
+    with open(path) as f:
+        lines = f.read().split("\n")
+    if lines and lines[-1] == "":
+        lines.pop()
+    assert len(lines) % 4 == 0
+    idx = [int(lines[k]) for k in range(0, len(lines), 4)]
+    xyz = [[float(lines[k + c]) for c in (1, 2, 3)] for k in range(0, len(lines), 4)]
+    return lines, idx, xyz
+
+
+def test_xyz_solution_file_content(tmp_path, oracle_mod):
+    """`lulesh_b200 -s 10 x 20` writes the node coordinates of cycle 20 in
+    the reference's format: 10-wide index lines and %.10f values, equal to
+    the oracle's coordinates to the printed precision; and the same file the
+    reference CUDA build writes (its 17-digit print hook) to 1e-9."""
+    r = _run("-s", "10", "x", "20", cwd=tmp_path)
+    assert r.returncode == 0, r.stdout + r.stderr
+    lines, idx, xyz = _read_xyz(tmp_path / "xyz.asc")
+    nn = 11 ** 3
+    assert idx == list(range(nn))
+    assert all(len(lines[k]) == 10 for k in range(0, len(lines), 4))
+    assert all(re.fullmatch(r"-?\d+\.\d{10}", lines[k + c])
+               for k in range(0, len(lines), 4) for c in (1, 2, 3))
+    o = oracle_mod.Oracle(10)
+    st, n = o.run(20)
+    assert st == 0 and n == 20
+    ref = list(zip(o.field("x"), o.field("y"), o.field("z")))
+    for got, want in zip(xyz, ref):
+        for g, w in zip(got, want):
+            assert abs(g - w) <= 5.000001e-11
+    ref_bin = os.path.join(os.path.dirname(PKG), "oracle", "_ref", "lulesh_ref_cuda")
+    if os.path.exists(ref_bin):
+        rd = tmp_path / "ref"
+        rd.mkdir()
+        rr = subprocess.run([ref_bin, "-s", "10", "x", "20"], capture_output=True, text=True,
+                            timeout=300, cwd=rd)
+        assert rr.returncode == 0, rr.stdout + rr.stderr
+        _, ridx, rxyz = _read_xyz(rd / "xyz.asc")
+        assert ridx == idx
+        for got, want in zip(xyz, rxyz):
+            for g, w in zip(got, want):
+                assert abs(g - w) <= 5.000001e-11 + 1e-9 * abs(w)
