@@ -462,17 +462,21 @@ int comm_prepare(lulesh_set *s)
 int enqueue_cycle_staged(lulesh_set *s)
 {
     cudaStream_t st = s->stream;
+    int r;
     launch_time_increment(s->dtc, s->njobs, s->P, st, s->pdl);
+    if ((r = cuda_status(cudaGetLastError(), "staged time increment")) != LULESH_OK) return r;
     launch_force_fp64(s, st);
+    if ((r = cuda_status(cudaGetLastError(), "staged force")) != LULESH_OK) return r;
     // AddNodeForcesFromElems over local corners only, then SBN exchange
     launch_nodal_gather_local(s->args(s->node_blocks), s->n_node_blocks, st);
+    if ((r = cuda_status(cudaGetLastError(), "staged local node sums")) != LULESH_OK) return r;
     FieldList f3{3, {LULESH_F_FX, LULESH_F_FY, LULESH_F_FZ}};
-    int r;
     if (s->tp > 1) {
         if ((r = comm_send_impl(s, -1, 3, f3, true, false, false, 1)) != LULESH_OK) return r;
         if ((r = comm_sbn_impl(s, -1, f3, 1)) != LULESH_OK) return r;
     }
     launch_nodal_update(s->args(s->node_blocks), s->n_node_blocks, s->P, st);
+    if ((r = cuda_status(cudaGetLastError(), "staged node update")) != LULESH_OK) return r;
     if (s->tp > 1) {
         FieldList f6{6, {LULESH_F_X, LULESH_F_Y, LULESH_F_Z, LULESH_F_XD, LULESH_F_YD,
                          LULESH_F_ZD}};
@@ -480,6 +484,7 @@ int enqueue_cycle_staged(lulesh_set *s)
         if ((r = comm_posvel_impl(s, -1, 1)) != LULESH_OK) return r;
     }
     launch_kinematics(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st);
+    if ((r = cuda_status(cudaGetLastError(), "staged kinematics")) != LULESH_OK) return r;
     if (s->tp > 1) {
         FieldList fq{3, {LULESH_F_DELV_XI, LULESH_F_DELV_ETA, LULESH_F_DELV_ZETA}};
         if ((r = comm_send_impl(s, -1, 3, fq, true, true, true, 1)) != LULESH_OK) return r;

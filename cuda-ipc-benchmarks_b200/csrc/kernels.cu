@@ -170,234 +170,9 @@ __global__ void __launch_bounds__(BS, min_blocks(kForceMinBlocks, BS)) k_force(S
     force_one<HG, U>(D, T, P, elem);
 }
 
-// ---------------------------------------------------------------------------
-// force, warp-specialised (structured meshes)
-//
-// One element's force splits into two chains that meet only at the end:
-//   stress     CalcElemShapeFunctionDerivatives (for the Jacobian check)
-//              and the face normals, giving -(sigma * B) per corner
-//   hourglass  the volume derivative, the four hourglass modes and the FB
-//              hourglass term coefficient * sum_m hourgam[k][m] * h[m]
-// A block of 2*TILE threads works on TILE elements: threads [0, TILE) (the
-// "stress" warps) compute the volume derivative, hand it over in shared
-// memory, then the stress; threads [TILE, 2*TILE) (the "hourglass" warps)
-// gather the velocities, take the volume derivative, form the modes and the
-// FB sums, and finally add the stress handed back through shared memory:
-// hgf = fma(coefficient, sum, stress), the contraction the one-thread form
-// makes.  Each role holds about half the registers of the whole element,
-// so twice as many warps are resident, and no warp diverges (TILE is a
-// multiple of 32, so a role is a whole warp).  Every FP64 expression keeps
-// its written form, so the corner forces are the one-thread kernel's bit
-// for bit.  Two named barriers order the hand-overs: the stress warps
-// arrive, the hourglass warps wait.
-#ifndef LULESH_FORCE_WS
-#define LULESH_FORCE_WS 1
-#endif
-
-__device__ __forceinline__ void named_bar_arrive(int id, int nthreads)
-{
-    asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
-}
-
-__device__ __forceinline__ void named_bar_sync(int id, int nthreads)
-{
-    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
-}
-
-// The mode sums hx/hy/hz[m] (the coordinates summed with mode m's signs)
-__device__ __forceinline__ void hourglass_mode_sums(const double (&xn)[8], const double (&yn)[8],
-                                                    const double (&zn)[8], double (&hx)[4],
-                                                    double (&hy)[4], double (&hz)[4])
-{
-#define LULESH_HG_SUM(a, s0, s1, s2, s3, s4, s5, s6, s7)                             \
-    (s0 a[0] s1 a[1] s2 a[2] s3 a[3] s4 a[4] s5 a[5] s6 a[6] s7 a[7])
-    hx[0] = LULESH_HG_SUM(xn, +, +, -, -, -, -, +, +);
-    hy[0] = LULESH_HG_SUM(yn, +, +, -, -, -, -, +, +);
-    hz[0] = LULESH_HG_SUM(zn, +, +, -, -, -, -, +, +);
-    hx[1] = LULESH_HG_SUM(xn, +, -, -, +, -, +, +, -);
-    hy[1] = LULESH_HG_SUM(yn, +, -, -, +, -, +, +, -);
-    hz[1] = LULESH_HG_SUM(zn, +, -, -, +, -, +, +, -);
-    hx[2] = LULESH_HG_SUM(xn, +, -, +, -, +, -, +, -);
-    hy[2] = LULESH_HG_SUM(yn, +, -, +, -, +, -, +, -);
-    hz[2] = LULESH_HG_SUM(zn, +, -, +, -, +, -, +, -);
-    hx[3] = LULESH_HG_SUM(xn, -, +, -, +, +, -, +, -);
-    hy[3] = LULESH_HG_SUM(yn, -, +, -, +, +, -, +, -);
-    hz[3] = LULESH_HG_SUM(zn, -, +, -, +, +, -, +, -);
-#undef LULESH_HG_SUM
-}
-
-// CalcHourglassModes (lulesh.cu:2017-2071) with the volume derivative read
-// from shared memory (dv[c*8 + k][t], c = x/y/z) and the mode sums formed
-// beforehand (hourglass_mode_sums): the same per-(corner, mode) expressions
-// as hourglass_modes, evaluated corner by corner
-__device__ __forceinline__ void hourglass_modes_staged(const double (&hx)[4],
-                                                       const double (&hy)[4],
-                                                       const double (&hz)[4],
-                                                       const double *dv, int stride,
-                                                       double (&hourgam)[8][4], double volinv)
-{
-    // the gamma sign patterns of the four modes, corner by corner
-    constexpr double g[4][8] = {{1.0, 1.0, -1.0, -1.0, -1.0, -1.0, 1.0, 1.0},
-                                {1.0, -1.0, -1.0, 1.0, -1.0, 1.0, 1.0, -1.0},
-                                {1.0, -1.0, 1.0, -1.0, 1.0, -1.0, 1.0, -1.0},
-                                {-1.0, 1.0, -1.0, 1.0, 1.0, -1.0, 1.0, -1.0}};
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const double dvx = dv[(0 * 8 + k) * stride];
-        const double dvy = dv[(1 * 8 + k) * stride];
-        const double dvz = dv[(2 * 8 + k) * stride];
-#pragma unroll
-        for (int m = 0; m < 4; ++m)
-            hourgam[k][m] = g[m][k] - volinv * (dvx * hx[m] + dvy * hy[m] + dvz * hz[m]);
-    }
-}
-
-// the FB sums of one velocity component (CalcElemFBHourglassForce,
-// lulesh.cu:1833-2013): sum[k] = sum_m hourgam[k][m] * (hourgam[:,m] . vel)
-__device__ __forceinline__ void fb_hourglass_sums(const double (&vel)[8],
-                                                  const double (&hourgam)[8][4],
-                                                  double (&sum)[8])
-{
-    double h[4];
-#pragma unroll
-    for (int m = 0; m < 4; ++m)
-        h[m] = hourgam[0][m] * vel[0] + hourgam[1][m] * vel[1] + hourgam[2][m] * vel[2] +
-               hourgam[3][m] * vel[3] + hourgam[4][m] * vel[4] + hourgam[5][m] * vel[5] +
-               hourgam[6][m] * vel[6] + hourgam[7][m] * vel[7];
-#pragma unroll
-    for (int k = 0; k < 8; ++k)
-        sum[k] = hourgam[k][0] * h[0] + hourgam[k][1] * h[1] + hourgam[k][2] * h[2] +
-                 hourgam[k][3] * h[3];
-}
-
-template <bool HG, int TILE>
-__global__ void __launch_bounds__(2 * TILE, (16 * 32) / (2 * TILE))
-    k_force_ws(SetArgs a, Params P)
-{
-    pdl_enter();
-    __shared__ double s_dv[24 * TILE];      // volume derivative, [c*8 + k][t]
-    __shared__ double s_stress[24 * TILE];  // -(sigma * B), [c*8 + k][t]
-    const int2 blk = a.blocks[LULESH_FORCE_REVERSE ? gridDim.x - 1 - blockIdx.x : blockIdx.x];
-    const DomDev &D = a.doms[blk.x];
-    TimeCtl &T = a.tcs[D.tc];
-    if (!T.active) return;  // uniform per block: before any barrier
-    const bool stress_role = threadIdx.x < TILE;
-    const int t = stress_role ? threadIdx.x : threadIdx.x - TILE;
-    const int elem = blk.y + t;
-    const bool valid = elem < D.numElem;
-    int n[8];
-    if (valid) {
-        elem_nodes<false>(D, elem, n);
-#pragma unroll
-        for (int i = 0; i < 8; ++i) n[i] = chk_index(n[i], D.numNode, &T, kChkNode);
-    }
-    if (stress_role) {
-        double xn[8], yn[8], zn[8];
-        if (valid) {
-#pragma unroll
-            for (int i = 0; i < 8; ++i) xn[i] = D.x[n[i]];
-#pragma unroll
-            for (int i = 0; i < 8; ++i) yn[i] = D.y[n[i]];
-#pragma unroll
-            for (int i = 0; i < 8; ++i) zn[i] = D.z[n[i]];
-            double dvdx[8], dvdy[8], dvdz[8];
-            elem_volume_derivative(dvdx, dvdy, dvdz, xn, yn, zn);
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                s_dv[(0 * 8 + k) * TILE + t] = dvdx[k];
-                s_dv[(1 * 8 + k) * TILE + t] = dvdy[k];
-                s_dv[(2 * 8 + k) * TILE + t] = dvdz[k];
-            }
-        }
-        named_bar_arrive(1, 2 * TILE);
-        if (valid) {
-            const double volume = D.v[elem];
-            double det = D.volo[elem] * volume;
-            if (volume < 0.) atomicMin(&T.bad_vol, elem);
-            const double sigxx = -D.p[elem] - D.q[elem];
-            double B[3][8];
-            shape_function_derivatives(xn, yn, zn, B, &det);
-            elem_node_normals(B[0], B[1], B[2], xn, yn, zn);
-            if (det < 0.) atomicMin(&T.bad_vol, elem);
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                s_stress[(0 * 8 + i) * TILE + t] = -(sigxx * B[0][i]);
-                s_stress[(1 * 8 + i) * TILE + t] = -(sigxx * B[1][i]);
-                s_stress[(2 * 8 + i) * TILE + t] = -(sigxx * B[2][i]);
-            }
-        }
-        named_bar_arrive(2, 2 * TILE);
-        return;
-    }
-    // hourglass role
-    double xdn[8], ydn[8], zdn[8];
-    double hx[4], hy[4], hz[4];
-    double coefficient = 0.0, volinv = 0.0;
-    if (valid) {
-        double xn[8], yn[8], zn[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            if (HG) {
-                xdn[i] = D.xd[n[i]];
-                ydn[i] = D.yd[n[i]];
-                zdn[i] = D.zd[n[i]];
-            }
-        }
-#pragma unroll
-        for (int i = 0; i < 8; ++i) xn[i] = D.x[n[i]];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) yn[i] = D.y[n[i]];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) zn[i] = D.z[n[i]];
-        hourglass_mode_sums(xn, yn, zn, hx, hy, hz);
-        const double det = D.volo[elem] * D.v[elem];
-        const double ss1 = D.ss[elem];
-        const double mass1 = D.elemMass[elem];
-        volinv = 1.0 / det;
-        const double hourg = P.hgcoef;
-        const double volume13 = cbrt(det);
-        coefficient = -hourg * 0.01 * ss1 * mass1 / volume13;
-    }
-    named_bar_sync(1, 2 * TILE);
-    double sx[8], sy[8], sz[8];
-    if (valid && HG) {
-        double hourgam[8][4];
-        hourglass_modes_staged(hx, hy, hz, s_dv + t, TILE, hourgam, volinv);
-        fb_hourglass_sums(xdn, hourgam, sx);
-        fb_hourglass_sums(ydn, hourgam, sy);
-        fb_hourglass_sums(zdn, hourgam, sz);
-    }
-    named_bar_sync(2, 2 * TILE);
-    if (!valid) return;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        double fx = s_stress[(0 * 8 + k) * TILE + t];
-        double fy = s_stress[(1 * 8 + k) * TILE + t];
-        double fz = s_stress[(2 * 8 + k) * TILE + t];
-        if (HG) {
-            fx = __fma_rn(coefficient, sx[k], fx);
-            fy = __fma_rn(coefficient, sy[k], fy);
-            fz = __fma_rn(coefficient, sz[k], fz);
-        }
-        const int c = elem + D.Ep * k;
-        st_corner(D.fx_elem + c, fx);
-        st_corner(D.fy_elem + c, fy);
-        st_corner(D.fz_elem + c, fz);
-    }
-}
-
 template <int BS, bool U = false>
 static void launch_force_bs(const SetArgs &a, int nblocks, Params P, cudaStream_t s)
 {
-    if constexpr (LULESH_FORCE_WS && !U && BS <= 128) {
-        // BS elements per block, 2*BS threads (static shared memory: 384 B
-        // per element, at most 48 KB)
-        if (P.hgcoef > 0.0)
-            launch_k(k_force_ws<true, BS>, nblocks, 2 * BS, s, a.pdl != 0, a, P);
-        else
-            launch_k(k_force_ws<false, BS>, nblocks, 2 * BS, s, a.pdl != 0, a, P);
-        return;
-    }
     if (P.hgcoef > 0.0)
         launch_k(k_force<true, BS, U>, nblocks, BS, s, a.pdl != 0, a, P);
     else
@@ -712,129 +487,9 @@ __global__ void __launch_bounds__(BS, min_blocks(kKinMinBlocks, BS)) k_kinematic
     kin_elem(D, T, k, x_local, y_local, z_local, vel);
 }
 
-// Kinematics, warp-specialised (structured meshes).  A block of 2*TILE
-// threads works on TILE elements; both roles gather the element's 48 node
-// values, then:
-//   volume role      CalcElemVolume -> vnew, delv (handing the volume over
-//                    in shared memory), the half-step shift and its undo,
-//                    CalcMonoGradient -> delx_*, delv_*
-//   divergence role  the six face areas, the half-step shift,
-//                    CalcElemShapeFunctionDerivatives and the velocity
-//                    divergence -> vdov, then (with the volume) the
-//                    characteristic length -> arealg
-// Each role keeps the written form of its expressions, so the outputs are
-// the one-thread kernel's bit for bit; each holds well under the 168
-// registers of the whole element.
-#ifndef LULESH_KIN_WS
-#define LULESH_KIN_WS 1
-#endif
-
-template <int TILE>
-__global__ void __launch_bounds__(2 * TILE, (16 * 32) / (2 * TILE)) k_kinematics_ws(SetArgs a)
-{
-    pdl_enter();
-    __shared__ double s_vol[TILE];
-    const int2 blk = a.blocks[LULESH_KIN_REVERSE ? gridDim.x - 1 - blockIdx.x : blockIdx.x];
-    const DomDev &D = a.doms[blk.x];
-    TimeCtl &T = a.tcs[D.tc];
-    if (!T.active) return;  // uniform per block: before the barrier
-    const bool volume_role = threadIdx.x < TILE;
-    const int t = volume_role ? threadIdx.x : threadIdx.x - TILE;
-    const int k = blk.y + t;
-    const bool valid = k < D.numElem;
-    double x_local[8], y_local[8], z_local[8];
-    double xd_local[8], yd_local[8], zd_local[8];
-    if (valid) {
-        int nodes[8];
-        elem_nodes<false>(D, k, nodes);
-#pragma unroll
-        for (int l = 0; l < 8; ++l) nodes[l] = chk_index(nodes[l], D.numNode, &T, kChkNode);
-#pragma unroll
-        for (int l = 0; l < 8; ++l) {
-            xd_local[l] = D.xd[nodes[l]];
-            yd_local[l] = D.yd[nodes[l]];
-            zd_local[l] = D.zd[nodes[l]];
-        }
-#pragma unroll
-        for (int l = 0; l < 8; ++l) x_local[l] = D.x[nodes[l]];
-#pragma unroll
-        for (int l = 0; l < 8; ++l) y_local[l] = D.y[nodes[l]];
-#pragma unroll
-        for (int l = 0; l < 8; ++l) z_local[l] = D.z[nodes[l]];
-    }
-    const double dt2 = 0.5 * T.deltatime;
-    if (volume_role) {
-        if (valid) {
-            const double volume = elem_volume(x_local, y_local, z_local);
-            s_vol[t] = volume;
-            const double relativeVolume = volume / D.volo[k];
-            D.vnew[k] = relativeVolume;
-            D.delv[k] = relativeVolume - D.v[k];
-            if (relativeVolume < 0) atomicMin(&T.bad_vol, k);
-            const double vol = D.volo[k] * relativeVolume;
-            // the half-step shift and its undo, as the one-thread form does
-            // them (the restored coordinates can differ in the last bit)
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                x_local[j] -= dt2 * xd_local[j];
-                y_local[j] -= dt2 * yd_local[j];
-                z_local[j] -= dt2 * zd_local[j];
-            }
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                x_local[j] += dt2 * xd_local[j];
-                y_local[j] += dt2 * yd_local[j];
-                z_local[j] += dt2 * zd_local[j];
-            }
-            double dxz, dvz, dxx, dvx, dxe, dve;
-            mono_gradient(x_local, y_local, z_local, xd_local, yd_local, zd_local, vol, &dxz,
-                          &dvz, &dxx, &dvx, &dxe, &dve);
-            D.delx_zeta[k] = dxz;
-            D.delv_zeta[k] = dvz;
-            D.delx_xi[k] = dxx;
-            D.delv_xi[k] = dvx;
-            D.delx_eta[k] = dxe;
-            D.delv_eta[k] = dve;
-        }
-        named_bar_arrive(1, 2 * TILE);
-        return;
-    }
-    // divergence role
-    double charLength = 0.0;
-    if (valid) {
-        charLength = fmax_t(area_face<double, 0, 1, 2, 3>(x_local, y_local, z_local), charLength);
-        charLength = fmax_t(area_face<double, 4, 5, 6, 7>(x_local, y_local, z_local), charLength);
-        charLength = fmax_t(area_face<double, 0, 1, 5, 4>(x_local, y_local, z_local), charLength);
-        charLength = fmax_t(area_face<double, 1, 2, 6, 5>(x_local, y_local, z_local), charLength);
-        charLength = fmax_t(area_face<double, 2, 3, 7, 6>(x_local, y_local, z_local), charLength);
-        charLength = fmax_t(area_face<double, 3, 0, 4, 7>(x_local, y_local, z_local), charLength);
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            x_local[j] -= dt2 * xd_local[j];
-            y_local[j] -= dt2 * yd_local[j];
-            z_local[j] -= dt2 * zd_local[j];
-        }
-        double B[3][8];
-        double Dv[3];
-        double detJ;
-        shape_function_derivatives(x_local, y_local, z_local, B, &detJ);
-        elem_velocity_divergence(xd_local, yd_local, zd_local, B, detJ, Dv);
-        D.vdov[k] = Dv[0] + Dv[1] + Dv[2];
-    }
-    named_bar_sync(1, 2 * TILE);
-    if (valid) D.arealg[k] = double(4.0) * s_vol[t] / sqrt_t(charLength);
-}
-
 void launch_kinematics(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs, bool u)
 {
     (void)P;
-    if (LULESH_KIN_WS && !u && (bs == 64 || bs == kElemBlock)) {
-        if (bs == 64)
-            launch_k(k_kinematics_ws<64>, nblocks, 128, s, a.pdl != 0, a);
-        else
-            launch_k(k_kinematics_ws<kElemBlock>, nblocks, 2 * kElemBlock, s, a.pdl != 0, a);
-        return;
-    }
     if (u) {
         launch_k(k_kinematics<kElemBlock, true>, nblocks, kElemBlock, s, a.pdl != 0, a);
         return;

@@ -349,3 +349,40 @@ def bench_decomposed(warmup: int, steps: int, dist, transport: str = "nccl") -> 
            "halo_bytes_per_cycle": 8 * part.halo_doubles()}
     part.close()
     return out
+
+
+def _main(argv=None) -> int:
+    """`python distributed.py --parts 8 --nx 32 --cycles 10`: every part of a
+    tp^3 problem on this process's GPU (LocalTransport, one stream), then
+    the origin energy next to the single-domain run's of the same mesh."""
+    import argparse
+    import json
+
+    import torch
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--parts", type=int, default=8)
+    ap.add_argument("--tp", type=int, default=2)
+    ap.add_argument("--nx", type=int, default=32, help="subdomain edge")
+    ap.add_argument("--cycles", type=int, default=10)
+    a = ap.parse_args(argv)
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        parts = [GpuPart(a.nx, a.tp, a.parts, p, stream=stream) for p in range(a.parts)]
+        eng = Engine(parts, LocalTransport())
+        eng.setup()
+        eng.run(a.cycles)
+    torch.cuda.synchronize()
+    e = parts[0].set.origin_energy()
+    with L.LuleshSet(nx=a.nx * a.tp, its=a.cycles) as single:
+        single.run()
+        e1 = single.origin_energy()
+    print(json.dumps({"parts": a.parts, "tp": a.tp, "nx": a.nx, "cycles": a.cycles,
+                      "origin_energy": e, "single_domain": e1, "equal": e == e1}))
+    for p in parts:
+        p.close()
+    return 0 if e == e1 else 1
+
+
+if __name__ == "__main__":
+    raise SystemExit(_main())
