@@ -78,6 +78,7 @@ EXPORTED = [
     "lulesh_part_of", "lulesh_halo_peers", "lulesh_halo_plan", "lulesh_create_part",
     "lulesh_part_finish_setup", "lulesh_halo_count", "lulesh_halo_pack", "lulesh_halo_unpack",
     "lulesh_part_phase", "lulesh_part_dt_pack", "lulesh_part_dt_unpack", "lulesh_wait_flag",
+    "lulesh_measure_fp64_peak",
 ]
 # the host-only planning functions, also exported by liblulesh_host.so
 HOST_PLAN_SIGS = {
@@ -215,6 +216,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "lulesh_part_dt_pack": (ip, [vp, vp]),
         "lulesh_part_dt_unpack": (ip, [vp, vp]),
         "lulesh_wait_flag": (ip, [vp, vp, ctypes.c_uint, dp]),
+        "lulesh_measure_fp64_peak": (ip, [ip, ctypes.POINTER(dp)]),
     }
     sig.update(HOST_PLAN_SIGS)
     for name, (res, args) in sig.items():
@@ -244,6 +246,15 @@ class JobSpec:
 
     def c(self) -> Job:
         return Job(self.nx, self.numReg, self.balance, self.cost, self.its)
+
+
+def measure_fp64_peak(device: int = -1) -> float:
+    """Measured FP64 FMA operations per second of the GPU
+    (lulesh_measure_fp64_peak)."""
+    lib = load_library()
+    v = ctypes.c_double()
+    _check(lib, lib.lulesh_measure_fp64_peak(device, ctypes.byref(v)), "lulesh_measure_fp64_peak")
+    return v.value
 
 
 def footprint_bytes(jobs: list[JobSpec], tp: int = 1) -> int:

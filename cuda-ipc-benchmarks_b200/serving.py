@@ -116,26 +116,33 @@ def run_plain(stream, device=0):
     return out, energy
 
 
-def plain_capacity(stream, repeats: int = 3, every: int = 10, device: int = 0) -> dict:
-    """The plain path's capacity, repeated: every `every`-th job of the
-    stream, all queued at t = 0, run job by job `repeats` times; capacity =
-    zone-cycles / summed service time of each repeat.  The per-job create
-    and destroy times of the plain path vary from run to run, so the median
-    is the figure to compare against."""
+def capacity_repeats(stream, repeats: int = 3, every: int = 10, device: int = 0,
+                     **kw) -> dict:
+    """Capacity of both forms on the same jobs, repeated: every `every`-th
+    job of the stream, all queued at t = 0, served `repeats` times and run
+    job by job `repeats` times.  Plain capacity = zone-cycles / summed
+    service time; served = zone-cycles / makespan.  The plain path's per-job
+    create and destroy times vary from run to run, so the medians are the
+    figures to compare."""
     sample = saturated(stream[::every])
-    caps = []
+    plain, served = [], []
     for _ in range(repeats):
         out, _ = run_plain(sample, device=device)
-        caps.append(out["capacity_zone_cycles_per_s"])
-    return {"jobs": len(sample), "every": every, "repeats": caps,
-            "median_zone_cycles_per_s": float(np.median(caps))}
+        plain.append(out["capacity_zone_cycles_per_s"])
+        srv, _ = run_served(sample, device=device, **kw)
+        served.append(srv["zone_cycles_per_s"])
+    pm, sm = float(np.median(plain)), float(np.median(served))
+    return {"jobs": len(sample), "every": every, "plain_repeats": plain,
+            "served_repeats": served, "plain_median_zone_cycles_per_s": pm,
+            "served_median_zone_cycles_per_s": sm, "capacity_ratio_median": sm / pm}
 
 
 def compare(stream, plain_repeats: int = 3, capacity_every: int = 10, **kw) -> dict:
     """Served vs plain on the same stream: at the offered load (arrival
     times kept) and at capacity (served: all jobs queued at t = 0; plain:
-    the median of `plain_repeats` capacity runs over a 1-in-`capacity_every`
-    sample, next to the capacity of the full offered-load run)."""
+    zone-cycles over the summed service times of its offered-load run), and
+    the capacity of both forms again, `plain_repeats` times each, over a
+    1-in-`capacity_every` sample (capacity_repeats)."""
     served, e_served = run_served(stream, **kw)
     sat, e_sat = run_served(saturated(stream), **kw)
     plain, e_plain = run_plain(stream, device=kw.get("device", 0))
@@ -146,10 +153,7 @@ def compare(stream, plain_repeats: int = 3, capacity_every: int = 10, **kw) -> d
            "capacity_ratio_full_run": sat["zone_cycles_per_s"] /
            plain["capacity_zone_cycles_per_s"],
            "energy_mismatches": mism}
+    out["capacity_ratio"] = out["capacity_ratio_full_run"]
     if plain_repeats > 0:
-        cap = plain_capacity(stream, plain_repeats, capacity_every, kw.get("device", 0))
-        out["plain_capacity"] = cap
-        out["capacity_ratio"] = sat["zone_cycles_per_s"] / cap["median_zone_cycles_per_s"]
-    else:
-        out["capacity_ratio"] = out["capacity_ratio_full_run"]
+        out["capacity_sample"] = capacity_repeats(stream, plain_repeats, capacity_every, **kw)
     return out

@@ -292,6 +292,13 @@ int lulesh_write_solution(lulesh_set *set, int domain, const char *path);
 const char *lulesh_status_string(int status);
 const char *lulesh_last_error(void);
 
+/* FP64 throughput of a GPU (device < 0: the current one), measured: fused
+ * multiply-adds per second (one FMA counts once) of independent
+ * register-only FMA chains over every SM, best of three timed launches.
+ * The denominator of the FP64 rooflines the benchmark reports.  No
+ * reference counterpart. */
+int lulesh_measure_fp64_peak(int device, double *fma_per_s);
+
 /* ---- serving: continuous batching of sedov jobs ----------------------- */
 /* No reference counterpart (the reference runs one job per process).  A
  * server owns one GPU stream.  Submitted jobs are meshed on host worker
