@@ -54,8 +54,6 @@ size_t domain_bytes(const DomSizes &s, bool mixed)
     b += align256(4 * s.corner);        // nodeElemCornerList
     b += 3 * align256(4 * s.en2);       // symm*
     b += 3 * align256(4 * s.nr);        // regCSR, regReps, regSorted
-    b += align256(8 * kEinFields * s.E);  // EOS inputs in slot order
-    b += align256(4 * s.E);             // slotOf
     if (s.comm) b += align256(8 * s.comm);
     if (mixed) b += 3 * align256(4 * 8 * s.Ep);
     if (s.unstructured) b += align256(4 * s.N);  // nodeBC
@@ -72,27 +70,6 @@ long comm_buffer_doubles(int nx, int tp)
     const long edge = nx + 1;
     const long maxPlane = ((edge * edge + pad - 1) / pad) * pad;
     return 6 * maxPlane * 6 + 12 * maxPlane * 6 + 8 * pad;
-}
-
-// slotOf (the inverse of eosOrder) and the slot-ordered copies of the
-// element mass and reference volume that the EOS kernel reads
-__global__ void k_eos_slots(DomDev D)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= D.numElem) return;
-    const int z = D.eosOrder[i];
-    if (z < 0 || z >= D.numElem) return;
-    const size_t E = D.numElem;
-    D.slotOf[z] = i;
-    D.eos_in[kEinMass * E + i] = D.elemMass[z];
-    D.eos_in[kEinVolo * E + i] = D.volo[z];
-}
-
-int eos_slots_setup(const DomDev &D, cudaStream_t st)
-{
-    if (D.numElem <= 0) return LULESH_OK;
-    k_eos_slots<<<(D.numElem + 127) / 128, 128, 0, st>>>(D);
-    return cuda_status(cudaGetLastError(), "EOS slot tables");
 }
 
 template <typename T>
@@ -166,8 +143,6 @@ int upload_domain(const HostDomain &h, int tc, long comm_doubles, bool mixed, Ca
     D.nodeElemCornerList = cv.take<int>(z.corner);
     D.symmX = cv.take<int>(z.en2); D.symmY = cv.take<int>(z.en2); D.symmZ = cv.take<int>(z.en2);
     D.regCSR = cv.take<int>(z.nr); D.regReps = cv.take<int>(z.nr); D.regSorted = cv.take<int>(z.nr);
-    D.eos_in = cv.take<double>(kEinFields * z.E);
-    D.slotOf = cv.take<int>(z.E);
     if (z.comm) {
         D.commRecv = cv.take<double>(z.comm);
         D.commRecvLen = (long)z.comm;
@@ -207,7 +182,6 @@ int upload_domain(const HostDomain &h, int tc, long comm_doubles, bool mixed, Ca
         int *rp[] = {D.regNumList, D.regElemlist, D.regCSR, D.regReps, D.regSorted, D.eosOrder};
         for (size_t k = 0; k < sizeof(rp) / sizeof(rp[0]); ++k)
             if ((su = upload(rp[k], *rv[k], st)) != LULESH_OK) return su;
-        if ((su = eos_slots_setup(D, st)) != LULESH_OK) return su;
         DCHECK(cudaStreamSynchronize(st));
         *out = D;
         return LULESH_OK;
@@ -235,7 +209,6 @@ int upload_domain(const HostDomain &h, int tc, long comm_doubles, bool mixed, Ca
         if ((su = upload(ip[k], *iv[k], st)) != LULESH_OK) return su;
     if (h.unstructured && (su = upload(D.nodeBC, h.nodeBC, st)) != LULESH_OK) return su;
     if (z.ell && (su = upload(D.nodeCornerEll, h.nodeCornerEll, st)) != LULESH_OK) return su;
-    if ((su = eos_slots_setup(D, st)) != LULESH_OK) return su;
     // the host vectors must outlive the asynchronous copies
     DCHECK(cudaStreamSynchronize(st));
     *out = D;

@@ -50,11 +50,6 @@ int upload_domain(const HostDomain &h, int tc, long comm_doubles, bool mixed, Ca
 // host; e[0] = einit.  Asynchronous on `st`.
 int setup_geometry_on_device(const DomDev &D, double einit, cudaStream_t st);
 
-// Fill D.slotOf and the set-up part of D.eos_in (element mass and reference
-// volume in EOS slot order) from D.eosOrder, D.elemMass and D.volo.
-// Asynchronous on `st`.
-int eos_slots_setup(const DomDev &D, cudaStream_t st);
-
 // The time state of a job before its first cycle (lulesh.cu:1120-1132).
 TimeCtl initial_timectl(double deltatime, int its_cap);
 

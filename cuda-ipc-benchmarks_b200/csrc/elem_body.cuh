@@ -163,17 +163,9 @@ __device__ __forceinline__ void kin_elem(const DomDev &D, TimeCtl &T, int k, dou
     double Dv[3];
     const double volume = elem_volume(x_local, y_local, z_local);
     const double relativeVolume = volume / D.volo[k];
-    // the EOS kernel's copies, in its slot order
-    const size_t E = D.numElem;
-    double *const ein = D.eos_in + chk_index(D.slotOf[k], D.numElem, &T, kChkSlot);
-    const double delv = relativeVolume - D.v[k];
-    const double arealg = elem_characteristic_length(x_local, y_local, z_local, volume);
     D.vnew[k] = relativeVolume;
-    D.delv[k] = delv;
-    D.arealg[k] = arealg;
-    ein[kEinVnew * E] = relativeVolume;
-    ein[kEinDelv * E] = delv;
-    ein[kEinArealg * E] = arealg;
+    D.delv[k] = relativeVolume - D.v[k];
+    D.arealg[k] = elem_characteristic_length(x_local, y_local, z_local, volume);
 
     double xd_local[8], yd_local[8], zd_local[8];
     vel.fetch(xd_local, yd_local, zd_local);
@@ -189,7 +181,6 @@ __device__ __forceinline__ void kin_elem(const DomDev &D, TimeCtl &T, int k, dou
     elem_velocity_divergence(xd_local, yd_local, zd_local, B, detJ, Dv);
     const double vdovNew = Dv[0] + Dv[1] + Dv[2];
     D.vdov[k] = vdovNew;
-    ein[kEinVdov * E] = vdovNew;
 
     const double vol = D.volo[k] * relativeVolume;
     // undo the half-step shift exactly as the reference does (the restored
@@ -209,12 +200,6 @@ __device__ __forceinline__ void kin_elem(const DomDev &D, TimeCtl &T, int k, dou
     D.delv_xi[k] = dvx;
     D.delx_eta[k] = dxe;
     D.delv_eta[k] = dve;
-    ein[kEinDelxZeta * E] = dxz;
-    ein[kEinDelvZeta * E] = dvz;
-    ein[kEinDelxXi * E] = dxx;
-    ein[kEinDelvXi * E] = dvx;
-    ein[kEinDelxEta * E] = dxe;
-    ein[kEinDelvEta * E] = dve;
     if (relativeVolume < 0) atomicMin(&T.bad_vol, k);
 }
 

@@ -551,26 +551,24 @@ __device__ __forceinline__ void elem_face_links(const DomDev &D, int z, int &bc,
     }
 }
 
-// one direction of the monotonic limiter, lulesh.cu:3595-3624; `own` is the
-// element's own gradient delv[i], the neighbours come from the element-ordered
-// array
-__device__ __forceinline__ double mono_limiter(const double *delv, double own, int bc, int mmask,
+// one direction of the monotonic limiter, lulesh.cu:3595-3624
+__device__ __forceinline__ double mono_limiter(const double *delv, int i, int bc, int mmask,
                                                int msymm, int mfree, int pmask, int psymm,
                                                int pfree, int lm, int lp, double mult,
                                                double maxslope, double ptiny, int nlinks,
                                                TimeCtl *T)
 {
-    const double norm = 1. / (own + ptiny);
+    const double norm = 1. / (delv[i] + ptiny);
     double delvm, delvp;
     const int mb = bc & mmask, pb = bc & pmask;
     if (mb == msymm)
-        delvm = own;
+        delvm = delv[i];
     else if (mb == mfree)
         delvm = 0.0;
     else  // 0 or *_COMM: neighbour or ghost element
         delvm = delv[chk_index(lm, nlinks, T, kChkLink)];
     if (pb == psymm)
-        delvp = own;
+        delvp = delv[i];
     else if (pb == pfree)
         delvp = 0.0;
     else
@@ -705,37 +703,30 @@ __global__ void __launch_bounds__(BS, min_blocks(kEosMinBlocks, BS)) k_eos(SetAr
         } else {
             elem_face_links(D, zidx, bcMask, lxm, lxp, lem, lep, lzm, lzp);
         }
-        // this slot's kinematics outputs, element mass and reference volume:
-        // the slot-ordered copies (coalesced loads)
-        const size_t E = D.numElem;
-        const double *const ein = D.eos_in + i;
-        const double dvxi_z = ein[kEinDelvXi * E], dveta_z = ein[kEinDelvEta * E],
-                     dvzeta_z = ein[kEinDelvZeta * E];
         const double mult = P.monoq_limiter_mult, maxs = P.monoq_max_slope;
         const double phixi =
-            mono_limiter(D.delv_xi, dvxi_z, bcMask, XI_M, XI_M_SYMM, XI_M_FREE, XI_P, XI_P_SYMM,
+            mono_limiter(D.delv_xi, zidx, bcMask, XI_M, XI_M_SYMM, XI_M_FREE, XI_P, XI_P_SYMM,
                          XI_P_FREE, lxm, lxp, mult, maxs, ptiny, D.allElem, &T);
         const double phieta =
-            mono_limiter(D.delv_eta, dveta_z, bcMask, ETA_M, ETA_M_SYMM, ETA_M_FREE, ETA_P,
+            mono_limiter(D.delv_eta, zidx, bcMask, ETA_M, ETA_M_SYMM, ETA_M_FREE, ETA_P,
                          ETA_P_SYMM, ETA_P_FREE, lem, lep, mult, maxs, ptiny, D.allElem, &T);
         const double phizeta =
-            mono_limiter(D.delv_zeta, dvzeta_z, bcMask, ZETA_M, ZETA_M_SYMM, ZETA_M_FREE, ZETA_P,
+            mono_limiter(D.delv_zeta, zidx, bcMask, ZETA_M, ZETA_M_SYMM, ZETA_M_FREE, ZETA_P,
                          ZETA_P_SYMM, ZETA_P_FREE, lzm, lzp, mult, maxs, ptiny, D.allElem, &T);
-        const double vdov_z = ein[kEinVdov * E];
-        const double vnew_z = ein[kEinVnew * E];
-        const double volo_z = ein[kEinVolo * E];
+        const double vdov_z = D.vdov[zidx];
+        const double vnew_z = D.vnew[zidx];
         double qlin, qquad;
         if (vdov_z > 0.) {
             qlin = 0.;
             qquad = 0.;
         } else {
-            double delvxxi = dvxi_z * ein[kEinDelxXi * E];
-            double delvxeta = dveta_z * ein[kEinDelxEta * E];
-            double delvxzeta = dvzeta_z * ein[kEinDelxZeta * E];
+            double delvxxi = D.delv_xi[zidx] * D.delx_xi[zidx];
+            double delvxeta = D.delv_eta[zidx] * D.delx_eta[zidx];
+            double delvxzeta = D.delv_zeta[zidx] * D.delx_zeta[zidx];
             if (delvxxi > 0.) delvxxi = 0.;
             if (delvxeta > 0.) delvxeta = 0.;
             if (delvxzeta > 0.) delvxzeta = 0.;
-            const double rho = ein[kEinMass * E] / (volo_z * vnew_z);
+            const double rho = D.elemMass[zidx] / (D.volo[zidx] * vnew_z);
             qlin = -P.qlc_monoq * rho *
                    (delvxxi * (1. - phixi) + delvxeta * (1. - phieta) +
                     delvxzeta * (1. - phizeta));
@@ -776,7 +767,7 @@ __global__ void __launch_bounds__(BS, min_blocks(kEosMinBlocks, BS)) k_eos(SetAr
         const double q_temp = q_old_z;
         const double qq_temp = qquad;
         const double ql_temp = qlin;
-        const double delvc_temp = ein[kEinDelv * E];
+        const double delvc_temp = D.delv[zidx];
         double rho0 = P.refdens;
         // The reference's cost model: every rep re-evaluates the EOS from
         // the same inputs (the loop is pure), lulesh.cu:4045-4083.
@@ -831,7 +822,7 @@ __global__ void __launch_bounds__(BS, min_blocks(kEosMinBlocks, BS)) k_eos(SetAr
             if (dth > dtdvov) dth = dtdvov;
         }
         const double ss_tmp = ssTmp;
-        const double area_tmp = ein[kEinArealg * E];
+        const double area_tmp = D.arealg[zidx];
         double dtf = ss_tmp * ss_tmp;
         dtf += ((vdov_tmp < 0.) ? qqc2 * area_tmp * area_tmp * vdov_tmp * vdov_tmp : 0.);
         dtf = area_tmp / sqrt(dtf);

@@ -80,15 +80,6 @@ struct DomDev {
     int eosNumClass;
     int eosClassEnd[kMaxRepClasses];
     int eosClassRep[kMaxRepClasses];
-    // The EOS kernel's inputs in EOS slot order (slot i holds element
-    // eosOrder[i]), so that kernel reads them with coalesced loads:
-    // eos_in[f * numElem + slot] for f = the kEin* fields below.  The
-    // kinematics kernels write fields kEinVnew..kEinDelvZeta every cycle
-    // beside the element-ordered Domain arrays; kEinMass and kEinVolo are
-    // copied once at set-up (and again when lulesh_set_field changes
-    // them).  slotOf[element] is the inverse of eosOrder.
-    double *eos_in;
-    int *slotOf;
     // comm message buffers (staged exchange): receive buffer of this rank
     double *commRecv;
     long commRecvLen;
@@ -102,12 +93,6 @@ struct DomDev {
     // null when some node has more than 8 corners (the kernel then reads the
     // run from nodeElemCornerList)
     int *nodeCornerEll;
-};
-
-// fields of DomDev::eos_in
-enum : int {
-    kEinVnew = 0, kEinDelv, kEinVdov, kEinArealg, kEinDelxXi, kEinDelxEta, kEinDelxZeta,
-    kEinDelvXi, kEinDelvEta, kEinDelvZeta, kEinMass, kEinVolo, kEinFields
 };
 
 // Mixed-precision corner forces, FP32, layout of fx_elem ([8][Ep]).

@@ -237,14 +237,8 @@ __global__ void __launch_bounds__(kElemBlock, LULESH_MIXED_KIN_MINB)
     }
     const double volume = elem_volume(xd64, yd64, zd64);
     const double relativeVolume = volume / D.volo[k];
-    // the EOS kernel's copies, in its slot order
-    const size_t E = D.numElem;
-    double *const ein = D.eos_in + chk_index(D.slotOf[k], D.numElem, &T, kChkSlot);
-    const double delv = relativeVolume - D.v[k];
     D.vnew[k] = relativeVolume;
-    D.delv[k] = delv;
-    ein[kEinVnew * E] = relativeVolume;
-    ein[kEinDelv * E] = delv;
+    D.delv[k] = relativeVolume - D.v[k];
     // FP32: everything else, on coordinates relative to corner 0
     float xl[8], yl[8], zl[8];
 #pragma unroll
@@ -253,9 +247,7 @@ __global__ void __launch_bounds__(kElemBlock, LULESH_MIXED_KIN_MINB)
         yl[l] = (float)(yd64[l] - yd64[0]);
         zl[l] = (float)(zd64[l] - zd64[0]);
     }
-    const double arealg = (double)elem_characteristic_length(xl, yl, zl, (float)volume);
-    D.arealg[k] = arealg;
-    ein[kEinArealg * E] = arealg;
+    D.arealg[k] = (double)elem_characteristic_length(xl, yl, zl, (float)volume);
     const float dt2 = (float)(0.5 * T.deltatime);
     float xh[8], yh[8], zh[8];
 #pragma unroll
@@ -267,9 +259,7 @@ __global__ void __launch_bounds__(kElemBlock, LULESH_MIXED_KIN_MINB)
     float B[3][8], detJ, Dv[3];
     shape_function_derivatives(xh, yh, zh, B, &detJ);
     elem_velocity_divergence(xv, yv, zv, B, detJ, Dv);
-    const double vdov = (double)(Dv[0] + Dv[1] + Dv[2]);
-    D.vdov[k] = vdov;
-    ein[kEinVdov * E] = vdov;
+    D.vdov[k] = (double)(Dv[0] + Dv[1] + Dv[2]);
     const float vol = (float)(D.volo[k] * relativeVolume);
     float dxz, dvz, dxx, dvx, dxe, dve;
     mono_gradient(xl, yl, zl, xv, yv, zv, vol, &dxz, &dvz, &dxx, &dvx, &dxe, &dve);
@@ -279,12 +269,6 @@ __global__ void __launch_bounds__(kElemBlock, LULESH_MIXED_KIN_MINB)
     D.delv_xi[k] = dvx;
     D.delx_eta[k] = dxe;
     D.delv_eta[k] = dve;
-    ein[kEinDelxZeta * E] = dxz;
-    ein[kEinDelvZeta * E] = dvz;
-    ein[kEinDelxXi * E] = dxx;
-    ein[kEinDelvXi * E] = dvx;
-    ein[kEinDelxEta * E] = dxe;
-    ein[kEinDelvEta * E] = dve;
     if (relativeVolume < 0) atomicMin(&T.bad_vol, k);
 }
 

@@ -975,12 +975,6 @@ int lulesh_set_field(lulesh_set *s, int d, const char *name, const void *src, si
     }
     LCHECK(cudaStreamSynchronize(s->stream));
     LCHECK(cudaMemcpy(f.ptr, src, nbytes, cudaMemcpyHostToDevice));
-    if (std::strcmp(name, "volo") == 0 || std::strcmp(name, "elemMass") == 0) {
-        // the EOS kernel reads its slot-ordered copies
-        const int st = eos_slots_setup(s->hdoms[d], s->stream);
-        if (st != LULESH_OK) return st;
-        LCHECK(cudaStreamSynchronize(s->stream));
-    }
     return LULESH_OK;
 }
 
