@@ -619,7 +619,8 @@ def run_distributed(a, rank, world, local_rank):
     import distributed as D
 
     torch.cuda.set_device(local_rank)
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    backend = "gloo" if a.transport == "host" else "nccl"
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     try:
         res = D.bench_decomposed(a.warmup, a.steps, dist, transport=a.transport)
     finally:
@@ -716,8 +717,9 @@ def main():
                     help="skip the config-2 subdomain leg")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false",
                     help="skip the reference omp CPU baseline")
-    ap.add_argument("--transport", default="nccl", choices=["nccl", "host"],
-                    help="halo transport between GPUs when N > 1")
+    ap.add_argument("--transport", default="nccl", choices=["nccl", "host", "direct"],
+                    help="halo transport between GPUs when N > 1 (direct: peer stores into "
+                         "the neighbours' mailboxes, dt over NCCL)")
     a = ap.parse_args()
     if a.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -19,6 +19,7 @@
 //     proxies, both through pointer tables built once from the plan.
 #include <algorithm>
 #include <climits>
+#include <cstring>
 #include <set>
 
 #include "domain_dev.hpp"
@@ -112,6 +113,7 @@ __global__ void k_wait_flag(const volatile unsigned int *flag, unsigned int expe
     }
     T->status = LULESH_TIMEOUT;
     T->done = 1;
+    T->active = 0;
 }
 
 int grid_for(long long n)
@@ -150,6 +152,90 @@ bool check_part(lulesh_set *s, int kind, int peer, int *slot)
         return false;
     }
     return true;
+}
+
+// The mailbox of part `part`: the message of each (kind, sender) it
+// receives, in kind-major, ascending-sender order, each at a 256-byte
+// boundary, then one 32-bit arrival flag per (kind, sender) in the same
+// order.  Computed from the plan alone, so a sender finds its place in a
+// receiver's mailbox without asking it.
+struct MailboxLayout {
+    std::vector<int> peers;
+    std::vector<size_t> offset;  // bytes, [kind * peers.size() + slot]
+    std::vector<long long> count;
+    size_t flags = 0, bytes = 0;
+};
+
+MailboxLayout mailbox_layout(int nx, int tp, int nparts, int part)
+{
+    MailboxLayout L;
+    L.peers = halo_peers(tp, nparts, part);
+    std::vector<HaloItem> items;
+    size_t off = 0;
+    for (int kind = 0; kind < HALO_KINDS; ++kind)
+        for (int q : L.peers) {
+            halo_plan(nx, tp, nparts, q, part, kind, items);
+            L.offset.push_back(off);
+            L.count.push_back((long long)items.size());
+            off += align256(sizeof(double) * items.size());
+        }
+    L.flags = off;
+    L.bytes = off + align256(sizeof(unsigned int) * HALO_KINDS * L.peers.size());
+    return L;
+}
+
+// Direct transport, sender side: gather this part's message for one peer
+// and store it straight into the peer's mailbox (peer memory, NVLink), then
+// make the stores visible system-wide before the flag kernel runs.
+__global__ void k_halo_put(const double *const *__restrict__ src, double *dst, long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        dst[i] = *src[i];
+    __threadfence_system();
+}
+
+// ... then raise the arrival flag (after the put kernel completed, in
+// stream order)
+__global__ void k_flag_raise(unsigned int *flag, unsigned int value)
+{
+    __threadfence_system();
+    atomicExch_system(flag, value);
+}
+
+// Direct transport, receiver side: wait (bounded, in device time and in
+// polls) until the sender's flag reaches `expect`, then scatter the message
+// from this part's mailbox into the proxies.  On timeout the job stops with
+// LULESH_TIMEOUT and nothing is scattered.
+__global__ void k_halo_take(const volatile unsigned int *flag, unsigned int expect,
+                            unsigned long long budget_ns, long long max_polls,
+                            double *const *__restrict__ dst, const double *in, long long n,
+                            TimeCtl *T)
+{
+    __shared__ int arrived;
+    if (threadIdx.x == 0) {
+        arrived = 0;
+        const unsigned long long t0 = global_ns();
+        for (long long k = 0; k < max_polls; ++k) {
+            if (*flag >= expect) {
+                arrived = 1;
+                break;
+            }
+            if (global_ns() - t0 > budget_ns) break;
+            __nanosleep(500);
+        }
+        if (!arrived) {  // the rest of this cycle's kernels skip as well
+            T->status = LULESH_TIMEOUT;
+            T->done = 1;
+            T->active = 0;
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    if (!arrived) return;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        *dst[i] = in[i];
 }
 
 }  // namespace
@@ -249,6 +335,16 @@ int part_build(lulesh_set *s)
             st = upload_table(ptrs, &s->halo_recv[kind * np + i]);
             if (st != LULESH_OK) return st;
         }
+    // the mailbox of the direct transport (its own allocation, so that it
+    // can be exported to the peers' processes with cudaIpcGetMemHandle)
+    const MailboxLayout L = mailbox_layout(j.nx, tp, s->nparts, s->part);
+    s->mailbox_bytes = L.bytes;
+    int st = cuda_status(cudaMalloc(&s->mailbox, L.bytes), "mailbox");
+    if (st != LULESH_OK) return st;
+    st = cuda_status(cudaMemsetAsync(s->mailbox, 0, L.bytes, s->stream), "mailbox");
+    if (st != LULESH_OK) return st;
+    s->peer_mailbox.assign(np, nullptr);
+    s->peer_mailbox_ipc.assign(np, false);
     return LULESH_OK;
 }
 
@@ -261,6 +357,11 @@ void part_release(lulesh_set *s)
     s->halo_recv.clear();
     if (s->proxy_arena) cudaFree(s->proxy_arena);
     s->proxy_arena = nullptr;
+    for (size_t i = 0; i < s->peer_mailbox.size(); ++i)
+        if (s->peer_mailbox[i] && s->peer_mailbox_ipc[i]) cudaIpcCloseMemHandle(s->peer_mailbox[i]);
+    s->peer_mailbox.clear();
+    if (s->mailbox) cudaFree(s->mailbox);
+    s->mailbox = nullptr;
 }
 
 }  // namespace lulesh
@@ -357,6 +458,100 @@ int lulesh_part_dt_unpack(lulesh_set *s, const long long *dev_buf)
     if (!s || !dev_buf) return LULESH_INVALID_ARG;
     k_dt_unpack<<<1, 1, 0, s->stream>>>(s->dtc, dev_buf);
     return cuda_status(cudaGetLastError(), "dt unpack");
+}
+
+int lulesh_part_mailbox(lulesh_set *s, void **dev_ptr, size_t *bytes, void *ipc_handle)
+{
+    if (!s || !s->mailbox) {
+        set_error("lulesh_part_mailbox: not a part of a multi-GPU problem");
+        return LULESH_INVALID_ARG;
+    }
+    if (dev_ptr) *dev_ptr = s->mailbox;
+    if (bytes) *bytes = s->mailbox_bytes;
+    if (ipc_handle) {
+        cudaIpcMemHandle_t h;
+        const int st = cuda_status(cudaIpcGetMemHandle(&h, s->mailbox), "mailbox IPC handle");
+        if (st != LULESH_OK) return st;
+        std::memcpy(ipc_handle, &h, sizeof h);
+    }
+    return LULESH_OK;
+}
+
+int lulesh_part_set_peer_mailbox(lulesh_set *s, int peer, const void *dev_ptr,
+                                 const void *ipc_handle)
+{
+    int slot;
+    if (!check_part(s, 0, peer, &slot)) return LULESH_INVALID_ARG;
+    if ((dev_ptr == nullptr) == (ipc_handle == nullptr)) {
+        set_error("lulesh_part_set_peer_mailbox: give a device pointer or an IPC handle");
+        return LULESH_INVALID_ARG;
+    }
+    if (s->peer_mailbox[slot] && s->peer_mailbox_ipc[slot])
+        cudaIpcCloseMemHandle(s->peer_mailbox[slot]);
+    s->peer_mailbox[slot] = nullptr;
+    if (dev_ptr) {
+        s->peer_mailbox[slot] = const_cast<void *>(dev_ptr);
+        s->peer_mailbox_ipc[slot] = false;
+        return LULESH_OK;
+    }
+    cudaIpcMemHandle_t h;
+    std::memcpy(&h, ipc_handle, sizeof h);
+    void *p = nullptr;
+    const int st = cuda_status(cudaIpcOpenMemHandle(&p, h, cudaIpcMemLazyEnablePeerAccess),
+                               "open peer mailbox");
+    if (st != LULESH_OK) return st;
+    s->peer_mailbox[slot] = p;
+    s->peer_mailbox_ipc[slot] = true;
+    return LULESH_OK;
+}
+
+int lulesh_halo_put(lulesh_set *s, int kind, int peer, unsigned int seq)
+{
+    int slot;
+    if (!check_part(s, kind, peer, &slot)) return LULESH_INVALID_ARG;
+    if (!s->peer_mailbox[slot]) {
+        set_error("lulesh_halo_put: the peer's mailbox is not set");
+        return LULESH_INVALID_ARG;
+    }
+    const lulesh_set::HaloTable &t = s->halo_send[kind * s->peers.size() + slot];
+    // where this part's message lands in the peer's mailbox
+    const MailboxLayout L = mailbox_layout(s->jobs[0].nx, s->tp, s->nparts, peer);
+    int me = -1;
+    for (size_t i = 0; i < L.peers.size(); ++i)
+        if (L.peers[i] == s->part) me = (int)i;
+    const size_t idx = kind * L.peers.size() + me;
+    if (me < 0 || L.count[idx] != t.n) {
+        set_error("lulesh_halo_put: mailbox layout mismatch");
+        return LULESH_INVALID_ARG;
+    }
+    char *base = static_cast<char *>(s->peer_mailbox[slot]);
+    if (t.n > 0)
+        k_halo_put<<<grid_for(t.n), 256, 0, s->stream>>>(
+            t.ptrs, reinterpret_cast<double *>(base + L.offset[idx]), t.n);
+    unsigned int *flag = reinterpret_cast<unsigned int *>(base + L.flags) + idx;
+    k_flag_raise<<<1, 1, 0, s->stream>>>(flag, seq);
+    return cuda_status(cudaGetLastError(), "halo put");
+}
+
+int lulesh_halo_take(lulesh_set *s, int kind, int peer, unsigned int seq, double timeout_ms)
+{
+    int slot;
+    if (!check_part(s, kind, peer, &slot)) return LULESH_INVALID_ARG;
+    if (!(timeout_ms > 0.0) || timeout_ms > 60000.0) {
+        set_error("lulesh_halo_take: 0 < timeout_ms <= 60000");
+        return LULESH_INVALID_ARG;
+    }
+    const lulesh_set::HaloTable &t = s->halo_recv[kind * s->peers.size() + slot];
+    const MailboxLayout L = mailbox_layout(s->jobs[0].nx, s->tp, s->nparts, s->part);
+    const size_t idx = kind * L.peers.size() + slot;
+    char *base = static_cast<char *>(s->mailbox);
+    const unsigned int *flag = reinterpret_cast<const unsigned int *>(base + L.flags) + idx;
+    const unsigned long long ns = (unsigned long long)(timeout_ms * 1e6);
+    const long long max_polls = (long long)(timeout_ms * 2e3) * 4 + 1000;
+    k_halo_take<<<grid_for(t.n > 0 ? t.n : 1), 256, 0, s->stream>>>(
+        flag, seq, ns, max_polls, t.ptrs, reinterpret_cast<const double *>(base + L.offset[idx]),
+        t.n, s->dtc);
+    return cuda_status(cudaGetLastError(), "halo take");
 }
 
 int lulesh_wait_flag(lulesh_set *s, const unsigned int *dev_flag, unsigned int expect,

@@ -101,6 +101,14 @@ struct lulesh_set {
     };
     std::vector<int> peers;
     std::vector<HaloTable> halo_send, halo_recv;  // [kind * peers.size() + peer slot]
+    // direct transport: this part's mailbox (every message it receives, at
+    // the offsets of mailbox_layout, then one arrival flag per message) and
+    // the mailboxes of its peers (mapped through CUDA IPC, or device
+    // pointers of parts in the same process)
+    void *mailbox = nullptr;
+    size_t mailbox_bytes = 0;
+    std::vector<void *> peer_mailbox;  // by peer slot
+    std::vector<bool> peer_mailbox_ipc;
 
     // staged comm state: receive-buffer capacity per domain (doubles)
     long com_buf_doubles = 0;

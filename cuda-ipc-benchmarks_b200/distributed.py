@@ -24,6 +24,10 @@ Pieces:
                    send/recv and all_reduce on the host, host -> device
   LocalTransport   every part in this process (device copies); lets one GPU
                    run the whole multi-part path
+  DirectTransport  peer stores: each message is written by the sender's kernel
+                   straight into the receiver's mailbox (CUDA IPC across
+                   processes), with an arrival flag the receiver's kernel
+                   waits on for a bounded time
   Engine           the cycle: phases, the three exchanges, the dt reduction
 
 A rank that fails or never arrives makes the others' next exchange end with
@@ -250,6 +254,79 @@ class HostTransport:
         b.copy_(c)
 
 
+class DirectTransport:
+    """Peer stores (the reference's remote-pack IPC backend, with its tokens
+    in device memory): a sender's kernel writes each message straight into
+    the receiver's mailbox over peer memory and raises an arrival flag; the
+    receiver's kernel waits for the flag (at most timeout_ms, then the job
+    stops with LULESH_TIMEOUT) and scatters the message into its proxies.
+    No staging buffer and no copy engine between the kernels.
+
+    dist=None: every part is in this process (the mailboxes are plain device
+    pointers).  Otherwise one part per process: the mailboxes are exported
+    as CUDA IPC handles and exchanged with all_gather_object, and the dt
+    record is reduced with all_reduce(MIN) over `dist` (NCCL); that
+    reduction is also what makes reusing a mailbox next cycle safe."""
+
+    name = "direct"
+    handles_packing = True
+
+    def __init__(self, dist=None, timeout_ms: float = 5000.0):
+        self.dist = dist
+        self.timeout_ms = timeout_ms
+        self.seq = {k: 0 for k in KINDS}
+        self.connected = False
+
+    def _connect(self, parts) -> None:
+        lib = L.load_library()
+        if self.dist is None:
+            ptr = {}
+            for p in parts:
+                v = ctypes.c_void_p()
+                L._check(lib, lib.lulesh_part_mailbox(p.h, ctypes.byref(v), None, None),
+                         "lulesh_part_mailbox")
+                ptr[p.part] = v.value
+            for p in parts:
+                for q in p.peers:
+                    L._check(lib, lib.lulesh_part_set_peer_mailbox(p.h, q, ctypes.c_void_p(ptr[q]),
+                                                                  None),
+                             "lulesh_part_set_peer_mailbox")
+        else:
+            (p,) = parts
+            h = ctypes.create_string_buffer(64)
+            L._check(lib, lib.lulesh_part_mailbox(p.h, None, None, h), "lulesh_part_mailbox")
+            handles = [None] * self.dist.get_world_size()
+            self.dist.all_gather_object(handles, h.raw)
+            for q in p.peers:
+                hq = ctypes.create_string_buffer(handles[q], 64)
+                L._check(lib, lib.lulesh_part_set_peer_mailbox(p.h, q, None, hq),
+                         "lulesh_part_set_peer_mailbox")
+        self.connected = True
+
+    def exchange(self, kind, parts) -> None:
+        if not self.connected:
+            self._connect(parts)
+        lib = L.load_library()
+        self.seq[kind] += 1
+        seq = self.seq[kind]
+        for p in parts:
+            for q in p.peers:
+                if p.send[kind][q].numel():
+                    L._check(lib, lib.lulesh_halo_put(p.h, kind, q, seq), "lulesh_halo_put")
+        for p in parts:
+            for q in p.peers:
+                if p.recv[kind][q].numel():
+                    L._check(lib, lib.lulesh_halo_take(p.h, kind, q, seq, self.timeout_ms),
+                             "lulesh_halo_take")
+
+    def allreduce_min(self, bufs) -> None:
+        if self.dist is None:
+            LocalTransport().allreduce_min(bufs)
+        else:
+            (b,) = bufs
+            self.dist.all_reduce(b, op=self.dist.ReduceOp.MIN)
+
+
 # ---------------------------------------------------------------------------
 # the cycle
 
@@ -263,6 +340,9 @@ class Engine:
         self.transport = transport
 
     def exchange(self, kind: int) -> None:
+        if getattr(self.transport, "handles_packing", False):
+            self.transport.exchange(kind, self.parts)  # kernels store into peers directly
+            return
         for p in self.parts:
             p.pack(kind)
         self.transport.exchange(kind, self.parts)
@@ -325,7 +405,8 @@ def bench_decomposed(warmup: int, steps: int, dist, transport: str = "nccl") -> 
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     part = GpuPart(nx, tp, world, rank, stream=stream)
-    tr = NcclTransport(dist) if transport == "nccl" else HostTransport(dist)
+    tr = {"nccl": NcclTransport, "host": HostTransport,
+          "direct": DirectTransport}[transport](dist)
     dist.barrier()
     eng = Engine([part], tr)
     eng.setup()
@@ -338,7 +419,8 @@ def bench_decomposed(warmup: int, steps: int, dist, transport: str = "nccl") -> 
     eng.run(steps)
     t1.record(stream)
     torch.cuda.synchronize()
-    ms = torch.tensor([t0.elapsed_time(t1)], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    ms = torch.tensor([t0.elapsed_time(t1)], dtype=torch.float64, device=dev)
     dist.all_reduce(ms, op=dist.ReduceOp.MAX)
     st = part.set.state()
     energy = part.set.origin_energy() if part_of(0, tp, world) == rank else None
@@ -365,11 +447,12 @@ def _main(argv=None) -> int:
     ap.add_argument("--tp", type=int, default=2)
     ap.add_argument("--nx", type=int, default=32, help="subdomain edge")
     ap.add_argument("--cycles", type=int, default=10)
+    ap.add_argument("--transport", default="local", choices=["local", "direct"])
     a = ap.parse_args(argv)
     stream = torch.cuda.Stream()
     with torch.cuda.stream(stream):
         parts = [GpuPart(a.nx, a.tp, a.parts, p, stream=stream) for p in range(a.parts)]
-        eng = Engine(parts, LocalTransport())
+        eng = Engine(parts, LocalTransport() if a.transport == "local" else DirectTransport())
         eng.setup()
         eng.run(a.cycles)
     torch.cuda.synchronize()

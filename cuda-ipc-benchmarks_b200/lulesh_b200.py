@@ -78,7 +78,8 @@ EXPORTED = [
     "lulesh_part_of", "lulesh_halo_peers", "lulesh_halo_plan", "lulesh_create_part",
     "lulesh_part_finish_setup", "lulesh_halo_count", "lulesh_halo_pack", "lulesh_halo_unpack",
     "lulesh_part_phase", "lulesh_part_dt_pack", "lulesh_part_dt_unpack", "lulesh_wait_flag",
-    "lulesh_measure_fp64_peak",
+    "lulesh_measure_fp64_peak", "lulesh_part_mailbox", "lulesh_part_set_peer_mailbox",
+    "lulesh_halo_put", "lulesh_halo_take",
 ]
 # the host-only planning functions, also exported by liblulesh_host.so
 HOST_PLAN_SIGS = {
@@ -217,6 +218,10 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "lulesh_part_dt_unpack": (ip, [vp, vp]),
         "lulesh_wait_flag": (ip, [vp, vp, ctypes.c_uint, dp]),
         "lulesh_measure_fp64_peak": (ip, [ip, ctypes.POINTER(dp)]),
+        "lulesh_part_mailbox": (ip, [vp, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_size_t), vp]),
+        "lulesh_part_set_peer_mailbox": (ip, [vp, ip, vp, vp]),
+        "lulesh_halo_put": (ip, [vp, ip, ip, ctypes.c_uint]),
+        "lulesh_halo_take": (ip, [vp, ip, ip, ctypes.c_uint, dp]),
     }
     sig.update(HOST_PLAN_SIGS)
     for name, (res, args) in sig.items():

@@ -502,6 +502,34 @@ int lulesh_part_phase(lulesh_set *set, int phase);
 int lulesh_part_dt_pack(lulesh_set *set, long long *dev_buf);
 int lulesh_part_dt_unpack(lulesh_set *set, const long long *dev_buf);
 
+/* Direct transport (peer stores over NVLink): every part owns a mailbox
+ * that holds each message it receives plus one arrival flag per message;
+ * the sender's kernel stores its message straight into the receiver's
+ * mailbox and then raises the flag to a sequence number, and the receiver's
+ * kernel waits for that number (bounded) before scattering the message into
+ * its proxies.  This is the reference's remote-pack IPC backend with its
+ * token protocol (comm/comm_ipc_common.h:26-261, lulesh-comms-direct.cu:
+ * 241-404) with the tokens in device memory.  The mailbox layout follows
+ * from the plan, so a sender knows where its message lands.
+ *   lulesh_part_mailbox: this part's mailbox (device pointer, size) and,
+ *     if ipc_handle is not NULL, its cudaIpcMemHandle (64 bytes) for the
+ *     peers' processes;
+ *   lulesh_part_set_peer_mailbox: a peer's mailbox, as a device pointer
+ *     (parts in one process) or an IPC handle (opened with peer access);
+ *   lulesh_halo_put: enqueue the message of `kind` to `peer` and raise its
+ *     flag to `seq` (every exchange of a kind uses the next number, from 1);
+ *   lulesh_halo_take: enqueue the wait for `seq` from `peer` (at most
+ *     timeout_ms; on timeout the job stops with LULESH_TIMEOUT and nothing
+ *     is scattered) and the scatter.
+ * A mailbox is reused every cycle: a sender may put the next message of a
+ * kind only after the receiver has taken the previous one, which the
+ * per-cycle dt reduction (a collective over all parts) guarantees. */
+int lulesh_part_mailbox(lulesh_set *set, void **dev_ptr, size_t *bytes, void *ipc_handle);
+int lulesh_part_set_peer_mailbox(lulesh_set *set, int peer, const void *dev_ptr,
+                                 const void *ipc_handle);
+int lulesh_halo_put(lulesh_set *set, int kind, int peer, unsigned int seq);
+int lulesh_halo_take(lulesh_set *set, int kind, int peer, unsigned int seq, double timeout_ms);
+
 /* Bounded wait on a device flag for transports that signal arrival with a
  * flag the sender sets in this GPU's memory (peer stores): enqueues a
  * one-thread kernel that spins until *flag >= expect or timeout_ms has

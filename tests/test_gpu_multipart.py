@@ -113,3 +113,139 @@ def test_bounded_flag_wait_times_out_and_the_context_survives(lulesh):
         assert s.state()["status"] == lulesh.OK
         assert s.run() == lulesh.OK  # the context is usable
         assert s.state()["cycle"] == 5
+
+
+def _two_proc_worker(rank, port, nx, cycles, q):
+    import datetime
+    import os
+    import sys
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, os.path.join(os.path.dirname(here), "cuda-ipc-benchmarks_b200"))
+    try:
+        import torch
+        import torch.distributed as dist
+
+        import distributed as D
+
+        torch.cuda.set_device(0)
+        dist.init_process_group("gloo", rank=rank, world_size=2,
+                                timeout=datetime.timedelta(seconds=60))
+        stream = torch.cuda.Stream()
+        torch.cuda.set_stream(stream)
+        part = D.GpuPart(nx, 2, 2, rank, device=0, stream=stream)
+        eng = D.Engine([part], D.HostTransport(dist, timeout_s=60.0))
+        dist.barrier()
+        eng.setup()
+        eng.run(cycles)
+        torch.cuda.synchronize()
+        fields = {d: {f: part.set.field(f, d) for f in ELEM + NODE}
+                  for d in range(part.set.num_domains)}
+        st = part.set.state()
+        e0 = part.set.origin_energy() if rank == 0 else None
+        part.close()
+        dist.barrier()
+        dist.destroy_process_group()
+        q.put((rank, "ok", fields, st, e0))
+    except Exception as e:  # noqa: BLE001
+        q.put((rank, "error", repr(e)[:400], None, None))
+
+
+def test_two_processes_on_one_gpu_match_single_domain(lulesh):
+    """Two processes, each with its own GpuPart on this GPU, exchange their
+    halo messages and dt through the host transport over gloo: the hosts
+    wait on each other, no kernel waits on another.  The decomposed run
+    equals the single domain bit for bit."""
+    import os
+
+    import torch.multiprocessing as mp
+
+    nx, cycles = 6, 25
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 29700 + os.getpid() % 2000
+    procs = [ctx.Process(target=_two_proc_worker, args=(r, port, nx, cycles, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted([q.get(timeout=300) for _ in procs], key=lambda t: t[0])
+    for p in procs:
+        p.join(timeout=60)
+    assert [r[1] for r in res] == ["ok", "ok"], res
+    with lulesh.LuleshSet(nx=nx * 2, its=-1, device=0) as single:
+        single.step(cycles)
+        ref = {f: single.field(f) for f in ELEM + NODE}
+        e_ref = single.origin_energy()
+    assert res[0][4] == e_ref
+    import distributed as D
+    for rank, _, fields, st, _ in res:
+        assert st["cycle"] == cycles and st["status"] == 0
+        ranks = [q2 for q2 in range(8) if D.part_of(q2, 2, 2) == rank]
+        for d, f_d in fields.items():
+            ge, gn = _region(nx, 2, ranks[d])
+            for f in ELEM:
+                assert np.array_equal(f_d[f][:nx ** 3], ref[f][ge]), (rank, d, f)
+            for f in NODE:
+                assert np.array_equal(f_d[f], ref[f][gn]), (rank, d, f)
+
+
+@pytest.mark.parametrize("nparts", [2, 8])
+def test_direct_transport_parts_on_one_gpu(lulesh, nparts):
+    """The direct transport with every part in this process: each put kernel
+    stores its message into the receiver's mailbox and raises the flag
+    before the receiver's take kernel runs (one stream), so no wait spins.
+    The run equals the single domain bit for bit."""
+    torch = pytest.importorskip("torch")
+    import distributed as D
+
+    nx, tp, cycles = 6, 2, 30
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        parts = [D.GpuPart(nx, tp, nparts, p, device=0, stream=stream) for p in range(nparts)]
+        eng = D.Engine(parts, D.DirectTransport())
+        eng.setup()
+        eng.run(cycles)
+    torch.cuda.synchronize()
+    with lulesh.LuleshSet(nx=nx * tp, its=-1, device=0) as single:
+        single.step(cycles)
+        ref = {f: single.field(f) for f in ELEM + NODE}
+        e_ref = single.origin_energy()
+    assert parts[0].set.origin_energy() == e_ref
+    for p in parts:
+        assert p.set.state()["status"] == 0 and p.set.state()["cycle"] == cycles
+        ranks = [q for q in range(tp ** 3) if D.part_of(q, tp, nparts) == p.part]
+        for d in range(p.set.num_domains):
+            ge, gn = _region(nx, tp, ranks[d])
+            for f in ELEM:
+                assert np.array_equal(p.set.field(f, d)[:nx ** 3], ref[f][ge]), (p.part, f)
+            for f in NODE:
+                assert np.array_equal(p.set.field(f, d), ref[f][gn]), (p.part, f)
+    for p in parts:
+        p.close()
+
+
+def test_direct_transport_take_that_never_arrives_times_out(lulesh):
+    """A take waiting for a sequence number no put has raised gives up after
+    its limit: the job stops with LULESH_TIMEOUT, nothing is scattered, and
+    the device keeps working."""
+    torch = pytest.importorskip("torch")
+    import distributed as D
+
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        parts = [D.GpuPart(4, 2, 2, p, device=0, stream=stream) for p in range(2)]
+        tr = D.DirectTransport(timeout_ms=200.0)
+        eng = D.Engine(parts, tr)
+        eng.setup()
+        eng.run(2)
+        lib = lulesh.load_library()
+        p = parts[1]
+        assert lib.lulesh_halo_take(p.h, lulesh.HALO_CORNERS, 0, 999, 200.0) == lulesh.OK
+    torch.cuda.synchronize()
+    st = parts[1].set.state()
+    assert st["status"] == lulesh.TIMEOUT and st["done"] == 1
+    assert parts[0].set.state()["status"] == lulesh.OK
+    for p in parts:
+        p.close()
+    with lulesh.LuleshSet(nx=4, its=3, device=0) as s:
+        assert s.run() == lulesh.OK
