@@ -618,7 +618,9 @@ def run_distributed(a, rank, world, local_rank):
     import torch.distributed as dist
     import distributed as D
 
-    torch.cuda.set_device(local_rank)
+    # one GPU per rank; with fewer GPUs than ranks (a test of the host
+    # transport on one GPU) ranks share devices round-robin
+    torch.cuda.set_device(local_rank % max(1, torch.cuda.device_count()))
     backend = "gloo" if a.transport == "host" else "nccl"
     dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     try:
