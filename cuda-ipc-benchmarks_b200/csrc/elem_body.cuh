@@ -131,34 +131,25 @@ __device__ __forceinline__ void force_elem_to(const DomDev &D, TimeCtl &T, const
     for (int k = 0; k < 8; ++k) store(k, hgfx[k], hgfy[k], hgfz[k]);
 }
 
-// the corner arrays at elem + Ep * corner; `keep` stores with the default
-// cache policy (read back from L2 soon), otherwise evict-first
+// the corner arrays at elem + Ep * corner
 struct CornerStore {
     const DomDev &D;
     int elem;
-    bool keep;
     __device__ __forceinline__ void operator()(int k, double fx, double fy, double fz) const
     {
         const int c = elem + D.Ep * k;
-        if (keep) {
-            D.fx_elem[c] = fx;
-            D.fy_elem[c] = fy;
-            D.fz_elem[c] = fz;
-        } else {
-            st_corner(D.fx_elem + c, fx);
-            st_corner(D.fy_elem + c, fy);
-            st_corner(D.fz_elem + c, fz);
-        }
+        st_corner(D.fx_elem + c, fx);
+        st_corner(D.fy_elem + c, fy);
+        st_corner(D.fz_elem + c, fz);
     }
 };
 
 template <bool HG, class Vel>
 __device__ __forceinline__ void force_elem(const DomDev &D, TimeCtl &T, const Params &P, int elem,
                                            const double (&xn)[8], const double (&yn)[8],
-                                           const double (&zn)[8], const Vel &vel,
-                                           bool keep = false)
+                                           const double (&zn)[8], const Vel &vel)
 {
-    force_elem_to<HG>(D, T, P, elem, xn, yn, zn, vel, CornerStore{D, elem, keep});
+    force_elem_to<HG>(D, T, P, elem, xn, yn, zn, vel, CornerStore{D, elem});
 }
 
 // CalcKinematicsAndMonotonicQGradient_kernel (lulesh.cu:3343-3507) after

@@ -126,8 +126,7 @@ __device__ __constant__ int kCZ[8] = {0, 0, 0, 0, 1, 1, 1, 1};
 
 // one element of the force phase: the node gathers, then force_elem
 template <bool HG, bool U>
-__device__ __forceinline__ void force_one(const DomDev &D, TimeCtl &T, const Params &P, int elem,
-                                          bool keep)
+__device__ __forceinline__ void force_one(const DomDev &D, TimeCtl &T, const Params &P, int elem)
 {
     // all 48 node gathers are issued before any arithmetic: the velocity
     // loads then overlap the coordinate work instead of stalling the
@@ -155,7 +154,7 @@ __device__ __forceinline__ void force_one(const DomDev &D, TimeCtl &T, const Par
     for (int i = 0; i < 8; ++i) yn[i] = D.y[n[i]];
 #pragma unroll
     for (int i = 0; i < 8; ++i) zn[i] = D.z[n[i]];
-    force_elem<HG>(D, T, P, elem, xn, yn, zn, vel, keep);
+    force_elem<HG>(D, T, P, elem, xn, yn, zn, vel);
 }
 
 template <bool HG, int BS, bool U>
@@ -168,7 +167,7 @@ __global__ void __launch_bounds__(BS, min_blocks(kForceMinBlocks, BS)) k_force(S
     if (!T.active) return;
     const int elem = blk.y + threadIdx.x;
     if (elem >= D.numElem) return;
-    force_one<HG, U>(D, T, P, elem, a.corner_keep != 0);
+    force_one<HG, U>(D, T, P, elem);
 }
 
 template <int BS, bool U = false>

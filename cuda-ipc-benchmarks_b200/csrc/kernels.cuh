@@ -75,10 +75,6 @@ struct SetArgs {
     // launch with programmatic stream serialisation (host side only; the
     // kernels launched this way wait for the previous grid first)
     int pdl = 0;
-    // force: store the corner forces with the default cache policy (the
-    // nodal kernel reads them back from L2 right after a chunk) instead of
-    // evict-first
-    int corner_keep = 0;
 };
 
 // ---------------------------------------------------------------------------

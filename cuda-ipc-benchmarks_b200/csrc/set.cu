@@ -74,44 +74,6 @@ int build_tables(lulesh_set *s)
     }
     // node blocks last-to-first (LULESH_NODAL_REVERSE, set.hpp)
     if (LULESH_NODAL_REVERSE) std::reverse(nb.begin(), nb.end());
-    // chunks of a single structured FP64 domain: element blocks in runs of
-    // consecutive blocks; after chunk c's force, the nodes below the first
-    // element plane not yet complete (rounded down to a node-block boundary,
-    // so no block reaches into the next chunk) have all their corners
-    s->chunk_eb_first.clear();
-    s->chunk_eb_count.clear();
-    s->chunk_nb_first.clear();
-    s->chunk_nb_count.clear();
-    const bool chunkable = s->ndom == 1 && s->tp == 1 && !s->unstructured &&
-                           !(s->flags & (LULESH_FLAG_MIXED | LULESH_FLAG_COMM_STAGED));
-    if (chunkable && s->nchunks > 1) {
-        const DomDev &D = s->hdoms[0];
-        const int neb = (int)eb.size(), per = (neb + s->nchunks - 1) / s->nchunks;
-        const long long plane = (long long)D.nx * D.nx, nplane = (long long)D.en * D.en;
-        std::vector<int2> nbc;
-        long long lo = 0;
-        for (int first = 0; first < neb; first += per) {
-            const int count = std::min(per, neb - first);
-            const bool last = first + count >= neb;
-            long long hi = D.numNode;
-            if (!last) {
-                const long long done = std::min<long long>(D.numElem, (long long)(first + count) * s->eb);
-                hi = (done / plane) * nplane;     // nodes of complete element planes
-                hi = (hi / s->nb) * s->nb;        // whole node blocks
-                hi = std::max(hi, lo);
-            }
-            s->chunk_eb_first.push_back(first);
-            s->chunk_eb_count.push_back(count);
-            s->chunk_nb_first.push_back((int)nbc.size());
-            std::vector<int2> part;
-            for (long long i = lo; i < hi; i += s->nb) part.push_back(make_int2(0, (int)i));
-            if (LULESH_NODAL_REVERSE) std::reverse(part.begin(), part.end());
-            nbc.insert(nbc.end(), part.begin(), part.end());
-            s->chunk_nb_count.push_back((int)part.size());
-            lo = hi;
-        }
-        nb.swap(nbc);  // every node exactly once, chunk by chunk
-    }
     s->n_elem_blocks = (int)eb.size();
     s->n_node_blocks = (int)nb.size();
     s->n_ghost_blocks = (int)gb.size();
@@ -296,34 +258,12 @@ void launch_force_fp64(lulesh_set *s, cudaStream_t st)
     launch_force(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb, s->unstructured);
 }
 
-// force and nodal chunk by chunk (lulesh_set_chunks): chunk c's corner
-// forces are still in L2 when its nodes are summed
-static void launch_force_nodal_chunked(lulesh_set *s, cudaStream_t st)
-{
-    for (size_t c = 0; c < s->chunk_eb_first.size(); ++c) {
-        SetArgs fa = s->args(s->elem_blocks + s->chunk_eb_first[c]);
-        fa.corner_keep = 1;
-        launch_force(fa, s->chunk_eb_count[c], s->P, st, s->eb, false);
-        if (s->chunk_nb_count[c] > 0)
-            launch_nodal(s->args(s->node_blocks + s->chunk_nb_first[c]), s->chunk_nb_count[c],
-                         s->P, st, s->nb, false);
-    }
-}
-
-static bool chunked(const lulesh_set *s) { return !s->chunk_eb_first.empty(); }
-
 int enqueue_cycle(lulesh_set *s)
 {
     if (s->flags & LULESH_FLAG_COMM_STAGED) return enqueue_cycle_staged(s);
     cudaStream_t st = s->stream;
     const bool mixed = (s->flags & LULESH_FLAG_MIXED) != 0;
     launch_time_increment(s->dtc, s->njobs, s->P, st, s->pdl);
-    if (chunked(s)) {
-        launch_force_nodal_chunked(s, st);
-        launch_kinematics(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb, false);
-        launch_eos(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb, false);
-        return cuda_status(cudaGetLastError(), "cycle launch");
-    }
     if (mixed)
         launch_force_mixed(s->args(s->elem_blocks), s->n_elem_blocks, s->P, s->dcorner32, st);
     else
@@ -813,25 +753,6 @@ int lulesh_step(lulesh_set *s, int ncycles)
     return LULESH_OK;
 }
 
-int lulesh_set_chunks(lulesh_set *s, int nchunks)
-{
-    if (!s || nchunks < 1 || nchunks > 64) {
-        set_error("lulesh_set_chunks: 1 <= nchunks <= 64");
-        return LULESH_INVALID_ARG;
-    }
-    if (nchunks == s->nchunks) return LULESH_OK;
-    LCHECK(cudaStreamSynchronize(s->stream));
-    s->nchunks = nchunks;
-    drop_graph(s);
-    return build_tables(s);
-}
-
-int lulesh_get_chunks(const lulesh_set *s)
-{
-    if (!s) return LULESH_INVALID_ARG;
-    return s->chunk_eb_first.empty() ? 1 : (int)s->chunk_eb_first.size();
-}
-
 int lulesh_set_graph_cycles(lulesh_set *s, int k)
 {
     if (!s || k < 1 || k > 100000) return LULESH_INVALID_ARG;
@@ -924,45 +845,6 @@ int lulesh_profile_phases(lulesh_set *s, int ncycles, double *ms_out, int *nphas
         LCHECK(cudaEventRecord(ev[0], st));
         launch_time_increment(s->dtc, s->njobs, s->P, st, s->pdl);
         LCHECK(cudaEventRecord(ev[1], st));
-        if (chunked(s)) {
-            // force and nodal interleave: time each launch and add them up
-            std::vector<cudaEvent_t> ce(2 * s->chunk_eb_first.size() + 1);
-            for (auto &e : ce) LCHECK(cudaEventCreate(&e));
-            LCHECK(cudaEventRecord(ce[0], st));
-            for (size_t k = 0; k < s->chunk_eb_first.size(); ++k) {
-                SetArgs fa = s->args(s->elem_blocks + s->chunk_eb_first[k]);
-                fa.corner_keep = 1;
-                launch_force(fa, s->chunk_eb_count[k], s->P, st, s->eb, false);
-                LCHECK(cudaEventRecord(ce[2 * k + 1], st));
-                if (s->chunk_nb_count[k] > 0)
-                    launch_nodal(s->args(s->node_blocks + s->chunk_nb_first[k]),
-                                 s->chunk_nb_count[k], s->P, st, s->nb, false);
-                LCHECK(cudaEventRecord(ce[2 * k + 2], st));
-            }
-            LCHECK(cudaEventSynchronize(ce.back()));
-            for (size_t k = 0; k < s->chunk_eb_first.size(); ++k) {
-                float f = 0.f, n = 0.f;
-                LCHECK(cudaEventElapsedTime(&f, ce[2 * k], ce[2 * k + 1]));
-                LCHECK(cudaEventElapsedTime(&n, ce[2 * k + 1], ce[2 * k + 2]));
-                acc[1] += f;
-                acc[2] += n;
-            }
-            for (auto &e : ce) cudaEventDestroy(e);
-            LCHECK(cudaEventRecord(ev[3], st));
-            LCHECK(cudaEventRecord(ev[4], st));
-            launch_kinematics(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb, false);
-            LCHECK(cudaEventRecord(ev[5], st));
-            LCHECK(cudaEventRecord(ev[6], st));
-            launch_eos(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb, false);
-            LCHECK(cudaEventRecord(ev[7], st));
-            LCHECK(cudaEventSynchronize(ev[7]));
-            for (int k : {0, 4, 6}) {
-                float ms = 0.f;
-                LCHECK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
-                acc[k] += ms;
-            }
-            continue;
-        }
         if (mixed)
             launch_force_mixed(s->args(s->elem_blocks), s->n_elem_blocks, s->P, s->dcorner32, st);
         else

@@ -46,14 +46,6 @@ struct lulesh_set {
     std::vector<lulesh_job> jobs;
     std::vector<size_t> corner_list_len;
 
-    // force/nodal chunks of a single structured FP64 domain
-    // (lulesh_set_chunks): chunk c runs the force blocks
-    // elem_blocks[chunk_eb_first[c] ..+ chunk_eb_count[c]) and then the nodal
-    // blocks node_blocks[chunk_nb_first[c] ..+ chunk_nb_count[c]), the nodes
-    // whose elements are all done by then; 1 = the unchunked cycle
-    int nchunks = 1;
-    std::vector<int> chunk_eb_first, chunk_eb_count, chunk_nb_first, chunk_nb_count;
-
     // block shapes and block-table order (lulesh_set_tuning): elements per
     // block of the FP64 element kernels, nodes per block of the nodal
     // kernel, 0 = domains in creation order / 1 = largest domain first

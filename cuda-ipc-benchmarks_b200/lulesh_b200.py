@@ -79,7 +79,7 @@ EXPORTED = [
     "lulesh_part_finish_setup", "lulesh_halo_count", "lulesh_halo_pack", "lulesh_halo_unpack",
     "lulesh_part_phase", "lulesh_part_dt_pack", "lulesh_part_dt_unpack", "lulesh_wait_flag",
     "lulesh_measure_fp64_peak", "lulesh_part_mailbox", "lulesh_part_set_peer_mailbox",
-    "lulesh_halo_put", "lulesh_halo_take", "lulesh_set_chunks", "lulesh_get_chunks",
+    "lulesh_halo_put", "lulesh_halo_take",
 ]
 # the host-only planning functions, also exported by liblulesh_host.so
 HOST_PLAN_SIGS = {
@@ -222,8 +222,6 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "lulesh_part_set_peer_mailbox": (ip, [vp, ip, vp, vp]),
         "lulesh_halo_put": (ip, [vp, ip, ip, ctypes.c_uint]),
         "lulesh_halo_take": (ip, [vp, ip, ip, ctypes.c_uint, dp]),
-        "lulesh_set_chunks": (ip, [vp, ip]),
-        "lulesh_get_chunks": (ip, [vp]),
     }
     sig.update(HOST_PLAN_SIGS)
     for name, (res, args) in sig.items():
@@ -350,13 +348,6 @@ class LuleshSet:
 
     def sync(self) -> None:
         _check(self.lib, self.lib.lulesh_sync(self.h), "lulesh_sync")
-
-    def set_chunks(self, n: int) -> None:
-        """Run force and nodal in n chunks (single structured FP64 domains)."""
-        _check(self.lib, self.lib.lulesh_set_chunks(self.h, n), "lulesh_set_chunks")
-
-    def chunks(self) -> int:
-        return int(self.lib.lulesh_get_chunks(self.h))
 
     def set_graph_cycles(self, k: int) -> None:
         _check(self.lib, self.lib.lulesh_set_graph_cycles(self.h, k), "lulesh_set_graph_cycles")

@@ -188,16 +188,6 @@ int lulesh_run_graph(lulesh_set *set, long long max_cycles);
  * one-cycle graph, so a whole batch run can be a single graph launch. */
 int lulesh_set_graph_cycles(lulesh_set *set, int k);
 
-/* Force/nodal chunking of a single structured FP64 domain (no reference
- * counterpart): the cycle runs the force kernel over `nchunks` runs of
- * consecutive element blocks, each followed by the nodal update of the
- * nodes whose elements are all done, so each chunk's corner forces are
- * still in L2 when they are summed.  Results do not depend on it (the same
- * work in another order).  1 = the unchunked cycle; other sets ignore it.
- * lulesh_get_chunks returns the chunks in use. */
-int lulesh_set_chunks(lulesh_set *set, int nchunks);
-int lulesh_get_chunks(const lulesh_set *set);
-
 /* Checkpoint of a set's whole state: every device array of every domain
  * and the time state of every job, behind a header that identifies the
  * set's jobs, subdomain count and flags.  No reference counterpart (the
