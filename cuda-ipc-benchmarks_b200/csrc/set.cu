@@ -381,10 +381,6 @@ static int ensure_graph_k(lulesh_set *s)
 
 void drop_graph(lulesh_set *s)
 {
-    if (s->exec_host) cudaGraphExecDestroy(s->exec_host);
-    if (s->graph_host) cudaGraphDestroy(s->graph_host);
-    s->exec_host = nullptr;
-    s->graph_host = nullptr;
     if (s->exec_k) cudaGraphExecDestroy(s->exec_k);
     if (s->graph_k) cudaGraphDestroy(s->graph_k);
     s->exec_k = nullptr;
@@ -805,35 +801,17 @@ int lulesh_host_cycle(lulesh_set *s, const lulesh_job_state *in, lulesh_job_stat
     int st = ensure_graph(s);
     if (st != LULESH_OK) return st;
     if (in) {
-        // host -> device: the time state the host decided on, the cycle and
-        // the record's way back as one graph launch (captured once)
-        if (!s->exec_host) {
-            LCHECK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-            cudaMemcpyAsync(&s->dtc[0].time, &s->htc_pinned[0].time, 2 * sizeof(double),
-                            cudaMemcpyHostToDevice, s->stream);
-            st = enqueue_cycle(s);
-            cudaMemcpyAsync(s->htc_pinned, s->dtc, sizeof(TimeCtl), cudaMemcpyDeviceToHost,
-                            s->stream);
-            cudaGraph_t g = nullptr;
-            const cudaError_t e = cudaStreamEndCapture(s->stream, &g);
-            if (st != LULESH_OK) {
-                if (g) cudaGraphDestroy(g);
-                return st;
-            }
-            LCHECK(e);
-            s->graph_host = g;
-            LCHECK(cudaGraphInstantiate(&s->exec_host, g, 0));
-        }
+        // host -> device: the time state the host decided on
         TimeCtl &T = s->htc_pinned[0];
         T.time = in->time;
         T.deltatime = in->deltatime;
-        LCHECK(cudaGraphLaunch(s->exec_host, s->stream));
-    } else {
-        LCHECK(cudaGraphLaunch(s->exec, s->stream));
-        // device -> host: the whole time-control record (dt, time, status)
-        LCHECK(cudaMemcpyAsync(s->htc_pinned, s->dtc, sizeof(TimeCtl), cudaMemcpyDeviceToHost,
-                               s->stream));
+        LCHECK(cudaMemcpyAsync(&s->dtc[0].time, &T.time, 2 * sizeof(double),
+                               cudaMemcpyHostToDevice, s->stream));
     }
+    LCHECK(cudaGraphLaunch(s->exec, s->stream));
+    // device -> host: the whole time-control record (dt, time, status)
+    LCHECK(cudaMemcpyAsync(s->htc_pinned, s->dtc, sizeof(TimeCtl), cudaMemcpyDeviceToHost,
+                           s->stream));
     LCHECK(cudaStreamSynchronize(s->stream));
     if (out) fill_state(s->htc_pinned[0], out);
     lulesh_job_state tmp;

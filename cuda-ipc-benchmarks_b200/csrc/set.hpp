@@ -78,10 +78,6 @@ struct lulesh_set {
     cudaGraph_t graph_k = nullptr;
     cudaGraphExec_t exec_k = nullptr;
     bool graph_k_ready = false;
-    // the host-driven cycle (lulesh_host_cycle): the time state copied in,
-    // one cycle, the time-control record copied out, as one graph
-    cudaGraph_t graph_host = nullptr;
-    cudaGraphExec_t exec_host = nullptr;
     // whole-run graph: a WHILE conditional node around one cycle
     // (rungraph.cu); run_ctl[0] counts cycles, run_ctl[1] is the cap
     cudaGraph_t graph_run = nullptr;
