@@ -58,8 +58,11 @@ def _summary(stream, lat, done_at, cycles, t0):
             "makespan_s": makespan, "zone_cycles": zc, "zone_cycles_per_s": zc / makespan}
 
 
-def run_served(stream, hbm_cap_bytes=150 * 10**9, max_jobs=512, cycles_per_step=64,
+def run_served(stream, hbm_cap_bytes=150 * 10**9, max_jobs=4096, cycles_per_step=64,
                prepare_threads=8, device=0):
+    """Serve `stream` through lulesh_server_*.  Admission is by device
+    footprint under hbm_cap_bytes; max_jobs (slots) is set above the
+    stream's size, so the footprint is what limits it."""
     srv = L.Server(hbm_cap_bytes=hbm_cap_bytes, max_jobs=max_jobs,
                    cycles_per_step=cycles_per_step, prepare_threads=prepare_threads,
                    device=device)
