@@ -391,10 +391,17 @@ class Engine:
 # ---------------------------------------------------------------------------
 # the N-GPU bench leg
 
-def bench_decomposed(warmup: int, steps: int, dist, transport: str = "nccl") -> dict:
+def bench_decomposed(warmup: int, steps: int, dist, transport: str = "nccl",
+                     clock=None) -> dict:
     """Each process (one per GPU) runs its part of a 2x2x2 (or larger cube)
     decomposition sized so every GPU holds about 1e6 elements; device time
-    of `steps` cycles after `warmup`, max over ranks."""
+    of `steps` cycles after `warmup`, max over ranks.  Then `steps` more
+    cycles driven from the host with each cycle's reduced dt record read
+    back to the host (32 bytes), timed on the host clock, max over ranks:
+    the end-to-end figure.  `clock` (start()/stop(), rank 0) samples the
+    GPU clocks over the device-timed cycles."""
+    import time
+
     import torch
 
     world, rank = dist.get_world_size(), dist.get_rank()
@@ -413,18 +420,32 @@ def bench_decomposed(warmup: int, steps: int, dist, transport: str = "nccl") -> 
     eng.run(warmup)
     torch.cuda.synchronize()
     dist.barrier()
+    if clock is not None:
+        clock.start()
+        time.sleep(0.3)  # the sampler is running before the timed cycles
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     t0.record(stream)
     eng.run(steps)
     t1.record(stream)
     torch.cuda.synchronize()
+    clocks = clock.stop() if clock is not None else None
     dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
     ms = torch.tensor([t0.elapsed_time(t1)], dtype=torch.float64, device=dev)
     dist.all_reduce(ms, op=dist.ReduceOp.MAX)
     st = part.set.state()
     energy = part.set.origin_energy() if part_of(0, tp, world) == rank else None
+    # end to end: the host drives every cycle and reads its result back
+    dist.barrier()
+    tw = time.perf_counter()
+    for _ in range(steps):
+        eng.cycle()
+        part.dt.cpu()
+    e2e_s = torch.tensor([time.perf_counter() - tw], dtype=torch.float64, device=dev)
+    dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
     out = {"ms_max_over_ranks": float(ms.item()), "sub_nx": nx, "tp": tp,
+           "e2e_s_max_over_ranks": float(e2e_s.item()), "e2e_d2h_bytes_per_step": 8 * 4,
+           "clocks": clocks,
            "global_nx": nx * tp, "zones_total": (nx * tp) ** 3, "transport": tr.name,
            "energy": energy, "cycle": st["cycle"], "status": st["status"],
            "launches_per_cycle": eng.launches_per_cycle(),
