@@ -509,7 +509,9 @@ def run_ours(a, rank, world, local_rank):
     ach_build = BUILD_BYTES_STEP * ZONES / (ms / a.steps / 1e3) / 1e9
 
     # end-to-end through the host-driven C-ABI call
-    e2e_n = min(a.steps, a.e2e_cycles)
+    # at least e2e_cycles host-driven cycles (a few tens of ms), so the
+    # figure does not rest on a handful of host round trips
+    e2e_n = max(a.steps, a.e2e_cycles)
     _, cur = s.host_cycle(None)
     tw = time.perf_counter()
     for _ in range(e2e_n):
@@ -705,7 +707,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--profile-cycles", dest="profile_cycles", type=int, default=5)
-    ap.add_argument("--e2e-cycles", dest="e2e_cycles", type=int, default=100)
+    ap.add_argument("--e2e-cycles", dest="e2e_cycles", type=int, default=200)
     ap.add_argument("--serve-jobs", dest="serve_jobs", type=int, default=2000,
                     help="jobs of the serving stream (2000 = the full stream; 0 skips)")
     ap.add_argument("--plain-repeats", dest="plain_repeats", type=int, default=3,
