@@ -225,6 +225,31 @@ def test_host_driven_cycle_matches_graph_run(lulesh):
         assert b.origin_energy() == ea
 
 
+def test_host_driven_cycle_takes_the_hosts_time_state(lulesh):
+    """The time state the host passes in is the one the cycle starts from:
+    moving the clock forward changes the trajectory, and the record handed
+    back is the device's after the cycle.  Plain steps and host cycles mix."""
+    with lulesh.LuleshSet(nx=10, its=-1) as a, lulesh.LuleshSet(nx=10, its=-1) as b:
+        a.step(3)
+        b.step(3)
+        _, oa = a.host_cycle(None)
+        _, ob = b.host_cycle(None)
+        assert (oa.time, oa.deltatime, oa.cycle) == (ob.time, ob.deltatime, ob.cycle) == (
+            oa.time, oa.deltatime, 4)
+        _, oa = a.host_cycle(oa)
+        moved = lulesh.JobState()
+        ctypes_fields = [f for f, _ in lulesh.JobState._fields_]
+        for f in ctypes_fields:
+            setattr(moved, f, getattr(ob, f))
+        moved.time = ob.time + 1.0e-4
+        _, ob = b.host_cycle(moved)
+        assert ob.cycle == oa.cycle == 5
+        assert ob.time > oa.time
+        st_a, st_b = a.state(), b.state()
+        assert st_a["time"] == oa.time and st_b["time"] == ob.time
+        assert st_a["deltatime"] == oa.deltatime and st_b["deltatime"] == ob.deltatime
+
+
 def test_profile_phases(lulesh):
     with lulesh.LuleshSet(nx=20, its=-1) as gs:
         ph = gs.profile_phases(3)
