@@ -22,13 +22,15 @@
 namespace lulesh {
 
 // Resident blocks per SM asked of the compiler for the mixed kernels:
-// 5 (96 registers) measured best on B200 at -s 100 (force 82 -> 78 us,
-// kinematics 70 -> 66 us against the unbounded build)
+// 4 (128 registers, no spills) measured best on B200 at -s 120, two
+// alternating runs each, identical results: force 137 us against 181 at 5
+// blocks (96 registers, spills), 147 at 3 and 311 at 6; kinematics 114.8 us
+// against 115.7 at 5 and 125.9 at 3; the cycle 498 us against 545 at 5.
 #ifndef LULESH_MIXED_FORCE_MINB
-#define LULESH_MIXED_FORCE_MINB 5
+#define LULESH_MIXED_FORCE_MINB 4
 #endif
 #ifndef LULESH_MIXED_KIN_MINB
-#define LULESH_MIXED_KIN_MINB 5
+#define LULESH_MIXED_KIN_MINB 4
 #endif
 
 __device__ __forceinline__ void elem_nodes_m(const DomDev &D, int el, int n[8])
