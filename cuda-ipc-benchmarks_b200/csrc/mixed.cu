@@ -142,7 +142,11 @@ __device__ __forceinline__ void comp_add(float &s, float &c, float v)
     s = t;
 }
 
-__global__ void __launch_bounds__(kNodeBlock, min_blocks(kNodalMinBlocks, kNodeBlock))
+#ifndef LULESH_MIXED_NODAL_MINB
+#define LULESH_MIXED_NODAL_MINB LULESH_NODAL_MINB
+#endif
+
+__global__ void __launch_bounds__(kNodeBlock, min_blocks(LULESH_MIXED_NODAL_MINB, kNodeBlock))
     k_nodal_mixed(SetArgs a, Params P, const CornerF32 *cfs)
 {
     pdl_enter();
