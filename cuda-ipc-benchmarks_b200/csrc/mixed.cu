@@ -162,16 +162,29 @@ __global__ void __launch_bounds__(kNodeBlock, min_blocks(LULESH_MIXED_NODAL_MINB
     float sx = 0.f, sy = 0.f, sz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
     const int ox[8] = {0, 1, 1, 0, 0, 1, 1, 0}, oy[8] = {0, 0, 1, 1, 0, 0, 1, 1},
               oz[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+    // all 24 corner loads first, then the compensated sums in corner order
+    float vx[8], vy[8], vz[8];
+    bool in[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         const int ex = px - ox[j], ey = py - oy[j], ez = pz - oz[j];
-        if ((unsigned)ex < (unsigned)nx && (unsigned)ey < (unsigned)nx &&
-            (unsigned)ez < (unsigned)nx) {
+        in[j] = (unsigned)ex < (unsigned)nx && (unsigned)ey < (unsigned)nx &&
+                (unsigned)ez < (unsigned)nx;
+        vx[j] = vy[j] = vz[j] = 0.f;
+        if (in[j]) {
             const int idx = chk_index(j * D.Ep + (ez * nx + ey) * nx + ex, 8LL * D.Ep,
                                       &a.tcs[D.tc], kChkCorner);
-            comp_add(sx, cx, __ldcs(cf.fx + idx));
-            comp_add(sy, cy, __ldcs(cf.fy + idx));
-            comp_add(sz, cz, __ldcs(cf.fz + idx));
+            vx[j] = __ldcs(cf.fx + idx);
+            vy[j] = __ldcs(cf.fy + idx);
+            vz[j] = __ldcs(cf.fz + idx);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        if (in[j]) {
+            comp_add(sx, cx, vx[j]);
+            comp_add(sy, cy, vy[j]);
+            comp_add(sz, cz, vz[j]);
         }
     }
     const double fx = (double)sx + (double)cx;
