@@ -205,23 +205,18 @@ __device__ __forceinline__ void gather_corners(const DomDev *doms, const DomDev 
                                                double &fz, TimeCtl *T)
 {
     const int nx = D.nx;
-    // every corner load is issued first, then the sums in corner order
-    double vx[8], vy[8], vz[8];
-    bool use[8];
+    fx = fy = fz = 0.0;
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         const int ex = px - kCX[j], ey = py - kCY[j], ez = pz - kCZ[j];
         const bool inside = (unsigned)ex < (unsigned)nx && (unsigned)ey < (unsigned)nx &&
                             (unsigned)ez < (unsigned)nx;
-        use[j] = false;
-        vx[j] = vy[j] = vz[j] = 0.0;
         if (inside) {
             const int idx = chk_index(j * D.Ep + (ez * nx + ey) * nx + ex, 8LL * D.Ep, T,
                                       kChkCorner);
-            vx[j] = ld_corner(D.fx_elem + idx);
-            vy[j] = ld_corner(D.fy_elem + idx);
-            vz[j] = ld_corner(D.fz_elem + idx);
-            use[j] = true;
+            fx += ld_corner(D.fx_elem + idx);
+            fy += ld_corner(D.fy_elem + idx);
+            fz += ld_corner(D.fz_elem + idx);
         } else if (D.tp > 1) {
             const int sx = (ex < 0) ? -1 : (ex >= nx ? 1 : 0);
             const int sy = (ey < 0) ? -1 : (ey >= nx ? 1 : 0);
@@ -232,20 +227,10 @@ __device__ __forceinline__ void gather_corners(const DomDev *doms, const DomDev 
                 const int lx = ex - sx * nx, ly = ey - sy * nx, lz = ez - sz * nx;
                 const int idx = chk_index(j * N.Ep + (lz * nx + ly) * nx + lx, 8LL * N.Ep,
                                           T, kChkCorner);
-                vx[j] = ld_corner(N.fx_elem + idx);
-                vy[j] = ld_corner(N.fy_elem + idx);
-                vz[j] = ld_corner(N.fz_elem + idx);
-                use[j] = true;
+                fx += ld_corner(N.fx_elem + idx);
+                fy += ld_corner(N.fy_elem + idx);
+                fz += ld_corner(N.fz_elem + idx);
             }
-        }
-    }
-    fx = fy = fz = 0.0;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        if (use[j]) {
-            fx += vx[j];
-            fy += vy[j];
-            fz += vz[j];
         }
     }
 }
