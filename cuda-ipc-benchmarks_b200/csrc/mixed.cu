@@ -143,7 +143,7 @@ __device__ __forceinline__ void comp_add(float &s, float &c, float v)
 }
 
 // Resident blocks per SM for the mixed node update, whose 24 corner loads
-// are all issued before the compensated sums: 10 (54 registers) measured
+// are all issued before the compensated sums: 10 (48 registers) measured
 // best on B200 at -s 120 (57.4 us against 57.7 at 8, 59.2 at 12 and 75.5
 // at 16; 83.7 us with the loads interleaved with the sums at 16).
 #ifndef LULESH_MIXED_NODAL_MINB
