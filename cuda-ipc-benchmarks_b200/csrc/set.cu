@@ -295,6 +295,10 @@ int enqueue_cycle(lulesh_set *s)
 #ifndef LULESH_L2_WINDOW
 #define LULESH_L2_WINDOW 1
 #endif
+// cap on the persisting lines in MB (0: the device's maximum)
+#ifndef LULESH_L2_PERSIST_MB
+#define LULESH_L2_PERSIST_MB 0
+#endif
 
 static int l2_node_window(lulesh_set *s)
 {
@@ -308,7 +312,9 @@ static int l2_node_window(lulesh_set *s)
     if (maxwin <= 0 || maxpersist <= 0) return LULESH_OK;
     size_t bytes = (size_t)(hi - lo);
     if (bytes > (size_t)maxwin) bytes = (size_t)maxwin;
-    const size_t persist = bytes < (size_t)maxpersist ? bytes : (size_t)maxpersist;
+    size_t persist = bytes < (size_t)maxpersist ? bytes : (size_t)maxpersist;
+    if (LULESH_L2_PERSIST_MB > 0 && persist > ((size_t)LULESH_L2_PERSIST_MB << 20))
+        persist = (size_t)LULESH_L2_PERSIST_MB << 20;
     // a limit of the process's context, released with it
     LCHECK(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, persist));
     cudaStreamAttrValue v{};
