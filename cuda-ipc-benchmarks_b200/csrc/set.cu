@@ -289,15 +289,14 @@ int enqueue_cycle(lulesh_set *s)
 // ~50 MB at -s 100, contiguous in the arena) persisting in L2: force reads
 // them, nodal reads and writes them, kinematics reads them again, every
 // cycle.  The access-policy window is a stream attribute, captured into
-// the cycle graph's kernel nodes.  Measured on B200 at -s 100: 339 -> 334
-// us per cycle.  Batches and subdomain sets do not use it.
+// the cycle graph's kernel nodes.  Only when those arrays take at most half
+// of the L2: measured on B200, the window takes -s 100 (49.5 MB) from 332.0
+// to 327.4 us per cycle, but -s 120 (85 MB) from 559.7 to 610.2 us (566.1
+// with the persisting lines capped at 48 MB); the results are the same.
+// Batches and subdomain sets do not use it.
 // 0 leaves every set's stream without an access-policy window
 #ifndef LULESH_L2_WINDOW
 #define LULESH_L2_WINDOW 1
-#endif
-// cap on the persisting lines in MB (0: the device's maximum)
-#ifndef LULESH_L2_PERSIST_MB
-#define LULESH_L2_PERSIST_MB 0
 #endif
 
 static int l2_node_window(lulesh_set *s)
@@ -306,15 +305,15 @@ static int l2_node_window(lulesh_set *s)
     const DomDev &D = s->hdoms[0];
     const char *lo = reinterpret_cast<const char *>(D.x);
     const char *hi = reinterpret_cast<const char *>(D.zd + D.numNode);
-    int maxwin = 0, maxpersist = 0;
+    int maxwin = 0, maxpersist = 0, l2 = 0;
     LCHECK(cudaDeviceGetAttribute(&maxwin, cudaDevAttrMaxAccessPolicyWindowSize, s->device));
     LCHECK(cudaDeviceGetAttribute(&maxpersist, cudaDevAttrMaxPersistingL2CacheSize, s->device));
-    if (maxwin <= 0 || maxpersist <= 0) return LULESH_OK;
+    LCHECK(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, s->device));
+    if (maxwin <= 0 || maxpersist <= 0 || l2 <= 0) return LULESH_OK;
     size_t bytes = (size_t)(hi - lo);
+    if (bytes > (size_t)l2 / 2) return LULESH_OK;
     if (bytes > (size_t)maxwin) bytes = (size_t)maxwin;
-    size_t persist = bytes < (size_t)maxpersist ? bytes : (size_t)maxpersist;
-    if (LULESH_L2_PERSIST_MB > 0 && persist > ((size_t)LULESH_L2_PERSIST_MB << 20))
-        persist = (size_t)LULESH_L2_PERSIST_MB << 20;
+    const size_t persist = bytes < (size_t)maxpersist ? bytes : (size_t)maxpersist;
     // a limit of the process's context, released with it
     LCHECK(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, persist));
     cudaStreamAttrValue v{};
