@@ -299,9 +299,44 @@ int enqueue_cycle(lulesh_set *s)
 #define LULESH_L2_WINDOW 1
 #endif
 
+// per device: sets holding a window, the persisting-L2 limit found before
+// the first and the one set now
+struct L2Limit {
+    int sets = 0;
+    size_t before = 0, now = 0;
+};
+static std::mutex g_l2_mu;
+static L2Limit g_l2[64];
+
+// Remove the window from the set's stream (it may be the caller's) and
+// release the lines it made persistent.
+static void clear_l2_window(lulesh_set *s)
+{
+    if (!s->l2_window || !s->stream) return;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != s->device) cudaSetDevice(s->device);
+    cudaStreamAttrValue v{};
+    v.accessPolicyWindow.num_bytes = 0;
+    cudaStreamSetAttribute(s->stream, cudaStreamAttributeAccessPolicyWindow, &v);
+    cudaCtxResetPersistingL2Cache();
+    {
+        std::lock_guard<std::mutex> lock(g_l2_mu);
+        L2Limit &g = g_l2[s->device];
+        if (--g.sets == 0) {
+            // the persisting share of L2 goes back to ordinary lines
+            cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, g.before);
+            g.now = g.before;
+        }
+    }
+    if (prev >= 0 && prev != s->device) cudaSetDevice(prev);
+    s->l2_window = false;
+}
+
 static int l2_node_window(lulesh_set *s)
 {
-    if (!LULESH_L2_WINDOW || s->ndom != 1) return LULESH_OK;
+    if (!LULESH_L2_WINDOW || s->ndom != 1 || s->device < 0 || s->device >= 64) return LULESH_OK;
+    if (s->l2_window) return LULESH_OK;  // already on the stream (graph rebuilt)
     const DomDev &D = s->hdoms[0];
     const char *lo = reinterpret_cast<const char *>(D.x);
     const char *hi = reinterpret_cast<const char *>(D.zd + D.numNode);
@@ -314,29 +349,34 @@ static int l2_node_window(lulesh_set *s)
     if (bytes > (size_t)l2 / 2) return LULESH_OK;
     if (bytes > (size_t)maxwin) bytes = (size_t)maxwin;
     const size_t persist = bytes < (size_t)maxpersist ? bytes : (size_t)maxpersist;
-    // a limit of the process's context, released with it
-    LCHECK(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, persist));
+    // a limit of the process's context: raised while any set on this device
+    // holds a window, and put back to what it was when the last one goes
+    {
+        std::lock_guard<std::mutex> lock(g_l2_mu);
+        L2Limit &g = g_l2[s->device];
+        if (g.sets == 0) {
+            LCHECK(cudaDeviceGetLimit(&g.before, cudaLimitPersistingL2CacheSize));
+            g.now = g.before;
+        }
+        if (persist > g.now) {
+            LCHECK(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, persist));
+            g.now = persist;
+        }
+        ++g.sets;
+        s->l2_window = true;  // counted: clear_l2_window undoes it
+    }
     cudaStreamAttrValue v{};
     v.accessPolicyWindow.base_ptr = const_cast<char *>(lo);
     v.accessPolicyWindow.num_bytes = bytes;
     v.accessPolicyWindow.hitRatio = (float)((double)persist / (double)bytes);
     v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
     v.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
-    LCHECK(cudaStreamSetAttribute(s->stream, cudaStreamAttributeAccessPolicyWindow, &v));
-    s->l2_window = true;
+    const cudaError_t e = cudaStreamSetAttribute(s->stream, cudaStreamAttributeAccessPolicyWindow, &v);
+    if (e != cudaSuccess) {
+        clear_l2_window(s);
+        return cuda_status(e, "cudaStreamSetAttribute(accessPolicyWindow)");
+    }
     return LULESH_OK;
-}
-
-// Remove the window from the set's stream (it may be the caller's) and
-// release the lines it made persistent.
-static void clear_l2_window(lulesh_set *s)
-{
-    if (!s->l2_window || !s->stream) return;
-    cudaStreamAttrValue v{};
-    v.accessPolicyWindow.num_bytes = 0;
-    cudaStreamSetAttribute(s->stream, cudaStreamAttributeAccessPolicyWindow, &v);
-    cudaCtxResetPersistingL2Cache();
-    s->l2_window = false;
 }
 
 static int ensure_graph(lulesh_set *s)
