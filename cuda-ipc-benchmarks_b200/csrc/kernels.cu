@@ -869,16 +869,34 @@ void launch_eos(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs,
 // CommSyncPosVel semantics (lulesh-comms-gpu.cu:1231-1661): a node shared by
 // several subdomains takes x,y,z,xd,yd,zd from the subdomain that holds it
 // on its minimum faces only (the "+side owner"), which never writes it here.
+// Blocks cover the max-side faces only (sync blocks, build_tables): block b
+// takes face blocks[b].y >> 24 of domain blocks[b].x from item
+// (blocks[b].y & 0xffffff) on.  Face 0 holds the nodes with px = nx, face 1
+// those with py = nx and px < nx, face 2 those with pz = nx and px, py < nx,
+// so every node of a max-side face is visited once; the copy itself is
+// decided from the node's position, as for the whole node range.
 __global__ void k_posvel_sync(SetArgs a)
 {
+    pdl_enter();
     const int2 blk = a.blocks[blockIdx.x];
     const DomDev &D = a.doms[blk.x];
     const TimeCtl &T = a.tcs[D.tc];
     if (!T.active) return;
-    const int i = blk.y + threadIdx.x;
-    if (i >= D.numNode) return;
+    const int face = blk.y >> 24;
+    const int item = (blk.y & 0xffffff) + threadIdx.x;
     const int en = D.en, nx = D.nx, tp = D.tp;
-    const int px = i % en, t = i / en, py = t % en, pz = t / en;
+    int px, py, pz;
+    if (face == 0) {
+        if (item >= en * en) return;
+        px = nx, py = item % en, pz = item / en;
+    } else if (face == 1) {
+        if (item >= nx * en) return;
+        px = item % nx, py = nx, pz = item / nx;
+    } else {
+        if (item >= nx * nx) return;
+        px = item % nx, py = item / nx, pz = nx;
+    }
+    const int i = (pz * en + py) * en + px;
     const int sx = (px == nx && D.col < tp - 1) ? 1 : 0;
     const int sy = (py == nx && D.row < tp - 1) ? 1 : 0;
     const int sz = (pz == nx && D.plane < tp - 1) ? 1 : 0;
@@ -898,7 +916,7 @@ __global__ void k_posvel_sync(SetArgs a)
 
 void launch_posvel_sync(const SetArgs &a, int nblocks, cudaStream_t s)
 {
-    k_posvel_sync<<<nblocks, kNodeBlock, 0, s>>>(a);
+    launch_k(k_posvel_sync, nblocks, kNodeBlock, s, a.pdl != 0, a);
 }
 
 // CommMonoQ semantics (lulesh-comms-gpu.cu:1665-1806): the delv_* ghost
@@ -907,6 +925,7 @@ void launch_posvel_sync(const SetArgs &a, int nblocks, cudaStream_t s)
 // of domain blocks[b].x, items (blocks[b].y & 0xffffff) onward.
 __global__ void k_monoq_ghost(SetArgs a)
 {
+    pdl_enter();
     const int2 blk = a.blocks[blockIdx.x];
     const DomDev &D = a.doms[blk.x];
     const TimeCtl &T = a.tcs[D.tc];
@@ -937,7 +956,7 @@ __global__ void k_monoq_ghost(SetArgs a)
 
 void launch_monoq_ghost(const SetArgs &a, int nblocks, cudaStream_t s)
 {
-    k_monoq_ghost<<<nblocks, kElemBlock, 0, s>>>(a);
+    launch_k(k_monoq_ghost, nblocks, kElemBlock, s, a.pdl != 0, a);
 }
 
 }  // namespace lulesh

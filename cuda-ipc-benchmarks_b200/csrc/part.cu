@@ -424,15 +424,15 @@ int lulesh_part_phase(lulesh_set *s, int phase)
     // plain stream order between phases: the transport's copies and
     // collectives sit between them on the same stream
     SetArgs ae = s->args(s->elem_blocks), an = s->args(s->node_blocks),
-            ag = s->args(s->ghost_blocks);
-    ae.pdl = an.pdl = ag.pdl = 0;
+            ag = s->args(s->ghost_blocks), as = s->args(s->sync_blocks);
+    ae.pdl = an.pdl = ag.pdl = as.pdl = 0;
     cudaStream_t st = s->stream;
     switch (phase) {
         case LULESH_PHASE_TIME_INCREMENT: launch_time_increment(s->dtc, s->njobs, s->P, st, false); break;
         case LULESH_PHASE_FORCE: launch_force(ae, s->n_elem_blocks, s->P, st, s->eb, false); break;
         case LULESH_PHASE_NODAL: launch_nodal(an, s->n_node_blocks, s->P, st, s->nb, false); break;
         case LULESH_PHASE_POSVEL_SYNC:
-            if (s->tp > 1) launch_posvel_sync(an, s->n_node_blocks, st);
+            if (s->tp > 1 && s->n_sync_blocks > 0) launch_posvel_sync(as, s->n_sync_blocks, st);
             break;
         case LULESH_PHASE_KINEMATICS:
             launch_kinematics(ae, s->n_elem_blocks, s->P, st, s->eb, false);

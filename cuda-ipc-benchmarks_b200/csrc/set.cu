@@ -61,23 +61,29 @@ int build_tables(lulesh_set *s)
         std::stable_sort(dord.begin(), dord.end(), [s](int a, int b) {
             return s->hdoms[a].numElem > s->hdoms[b].numElem;
         });
-    std::vector<int2> eb, nb, gb;
+    std::vector<int2> eb, nb, gb, sb;
     for (int d : dord) {
         const DomDev &D = s->hdoms[d];
         for (int i = 0; i < D.numElem; i += s->eb) eb.push_back(make_int2(d, i));
         for (int i = 0; i < D.numNode; i += s->nb) nb.push_back(make_int2(d, i));
-        if (D.tp > 1)
+        if (D.tp > 1) {
             for (int f = 0; f < 6; ++f)
                 if (D.ghost[f] >= 0)
                     for (int i = 0; i < D.nx * D.nx; i += kElemBlock)
                         gb.push_back(make_int2(d, (f << 24) | i));
+            // the max-side node faces (k_posvel_sync): en^2, nx*en, nx^2 nodes
+            const int items[3] = {D.en * D.en, D.nx * D.en, D.nx * D.nx};
+            for (int f = 0; f < 3; ++f)
+                for (int i = 0; i < items[f]; i += kNodeBlock) sb.push_back(make_int2(d, (f << 24) | i));
+        }
     }
     // node blocks last-to-first (LULESH_NODAL_REVERSE, set.hpp)
     if (LULESH_NODAL_REVERSE) std::reverse(nb.begin(), nb.end());
     s->n_elem_blocks = (int)eb.size();
     s->n_node_blocks = (int)nb.size();
     s->n_ghost_blocks = (int)gb.size();
-    size_t bytes = sizeof(int2) * (eb.size() + nb.size() + gb.size() + 1);
+    s->n_sync_blocks = (int)sb.size();
+    size_t bytes = sizeof(int2) * (eb.size() + nb.size() + gb.size() + sb.size() + 1);
     if (s->elem_blocks) {  // rebuilding: the old tables may still be in use
         LCHECK(cudaStreamSynchronize(s->stream));
         LCHECK(cudaFree(s->elem_blocks));
@@ -88,12 +94,16 @@ int build_tables(lulesh_set *s)
     s->elem_blocks = t;
     s->node_blocks = t + eb.size();
     s->ghost_blocks = t + eb.size() + nb.size();
+    s->sync_blocks = t + eb.size() + nb.size() + gb.size();
     LCHECK(cudaMemcpyAsync(s->elem_blocks, eb.data(), sizeof(int2) * eb.size(),
                            cudaMemcpyHostToDevice, s->stream));
     LCHECK(cudaMemcpyAsync(s->node_blocks, nb.data(), sizeof(int2) * nb.size(),
                            cudaMemcpyHostToDevice, s->stream));
     if (!gb.empty())
         LCHECK(cudaMemcpyAsync(s->ghost_blocks, gb.data(), sizeof(int2) * gb.size(),
+                               cudaMemcpyHostToDevice, s->stream));
+    if (!sb.empty())
+        LCHECK(cudaMemcpyAsync(s->sync_blocks, sb.data(), sizeof(int2) * sb.size(),
                                cudaMemcpyHostToDevice, s->stream));
     return LULESH_OK;
 }
@@ -273,7 +283,8 @@ int enqueue_cycle(lulesh_set *s)
     else
         launch_nodal(s->args(s->node_blocks), s->n_node_blocks, s->P, st, s->nb,
                          s->unstructured);
-    if (s->tp > 1) launch_posvel_sync(s->args(s->node_blocks), s->n_node_blocks, st);
+    if (s->tp > 1 && s->n_sync_blocks > 0)
+        launch_posvel_sync(s->args(s->sync_blocks), s->n_sync_blocks, st);
     if (mixed)
         launch_kinematics_mixed(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st);
     else
@@ -901,7 +912,8 @@ int lulesh_profile_phases(lulesh_set *s, int ncycles, double *ms_out, int *nphas
             launch_nodal(s->args(s->node_blocks), s->n_node_blocks, s->P, st, s->nb,
                          s->unstructured);
         LCHECK(cudaEventRecord(ev[3], st));
-        if (s->tp > 1) launch_posvel_sync(s->args(s->node_blocks), s->n_node_blocks, st);
+        if (s->tp > 1 && s->n_sync_blocks > 0)
+            launch_posvel_sync(s->args(s->sync_blocks), s->n_sync_blocks, st);
         LCHECK(cudaEventRecord(ev[4], st));
         if (mixed)
             launch_kinematics_mixed(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st);

@@ -57,6 +57,9 @@ struct lulesh_set {
     lulesh::TimeCtl *htc_pinned = nullptr;  // pinned mirror for readback
     int2 *elem_blocks = nullptr, *node_blocks = nullptr, *ghost_blocks = nullptr;
     int n_elem_blocks = 0, n_node_blocks = 0, n_ghost_blocks = 0;
+    // subdomain sets: blocks over the max-side node faces (PosVel sync)
+    int2 *sync_blocks = nullptr;
+    int n_sync_blocks = 0;
 
     // mixed precision corner buffers
     lulesh::CornerF32 *dcorner32 = nullptr;
