@@ -344,7 +344,22 @@ static void clear_l2_window(lulesh_set *s)
     s->l2_window = false;
 }
 
+static int l2_node_window_on_device(lulesh_set *s);
+
+// the limit and the stream attribute belong to the set's device: make it
+// current for the call, whatever device the calling thread has
 static int l2_node_window(lulesh_set *s)
+{
+    if (!LULESH_L2_WINDOW || s->ndom != 1 || s->l2_window) return LULESH_OK;
+    int prev = -1;
+    LCHECK(cudaGetDevice(&prev));
+    if (prev != s->device) LCHECK(cudaSetDevice(s->device));
+    const int st = l2_node_window_on_device(s);
+    if (prev != s->device) cudaSetDevice(prev);
+    return st;
+}
+
+static int l2_node_window_on_device(lulesh_set *s)
 {
     if (!LULESH_L2_WINDOW || s->ndom != 1 || s->device < 0 || s->device >= 64) return LULESH_OK;
     if (s->l2_window) return LULESH_OK;  // already on the stream (graph rebuilt)
