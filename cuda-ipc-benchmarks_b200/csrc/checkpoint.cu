@@ -15,7 +15,7 @@ namespace lulesh {
 namespace {
 
 constexpr unsigned kMagic = 0x4c554c43u;  // "LULC"
-constexpr unsigned kVersion = 2;
+constexpr unsigned kVersion = 3;  // 3: subdomain sets carve x..zd first
 
 struct CkptHeader {
     unsigned magic, version;

@@ -87,8 +87,10 @@ static int upload(T *dst, const std::vector<T> &src, cudaStream_t s)
         if (_st != LULESH_OK) return _st;                       \
     } while (0)
 
+size_t node_region_bytes(size_t numNode) { return 6 * align256(8 * numNode); }
+
 int upload_domain(const HostDomain &h, int tc, long comm_doubles, bool mixed, Carver &cv,
-                  cudaStream_t st, DomDev *out, CornerF32 *c32)
+                  cudaStream_t st, DomDev *out, CornerF32 *c32, Carver *node_cv)
 {
     const DomSizes z = sizes_of(h, comm_doubles);
     DomDev D{};
@@ -120,8 +122,9 @@ int upload_domain(const HostDomain &h, int tc, long comm_doubles, bool mixed, Ca
     D.delv_xi = cv.take<double>(z.allElem); D.delv_eta = cv.take<double>(z.allElem);
     D.delv_zeta = cv.take<double>(z.allElem);
     // node doubles
-    D.x = cv.take<double>(z.N); D.y = cv.take<double>(z.N); D.z = cv.take<double>(z.N);
-    D.xd = cv.take<double>(z.N); D.yd = cv.take<double>(z.N); D.zd = cv.take<double>(z.N);
+    Carver &ncv = node_cv ? *node_cv : cv;
+    D.x = ncv.take<double>(z.N); D.y = ncv.take<double>(z.N); D.z = ncv.take<double>(z.N);
+    D.xd = ncv.take<double>(z.N); D.yd = ncv.take<double>(z.N); D.zd = ncv.take<double>(z.N);
     D.xdd = cv.take<double>(z.N); D.ydd = cv.take<double>(z.N); D.zdd = cv.take<double>(z.N);
     D.fx = cv.take<double>(z.N); D.fy = cv.take<double>(z.N); D.fz = cv.take<double>(z.N);
     D.nodalMass = cv.take<double>(z.N);

@@ -42,8 +42,14 @@ struct Carver {
 // on `st`, and fill the device record *D (and *c32 when mixed).  `tc` is
 // the TimeCtl slot of the domain's job.  Synchronises `st` before
 // returning, so `h` may be released afterwards.
+// With node_cv, x, y, z, xd, yd and zd come from node_cv (a set's node
+// region: every domain's six arrays one after the other) and cv carves the
+// rest; cv then advances by node_region_bytes(...) less than domain_bytes.
 int upload_domain(const HostDomain &h, int tc, long comm_doubles, bool mixed, Carver &cv,
-                  cudaStream_t st, DomDev *D, CornerF32 *c32);
+                  cudaStream_t st, DomDev *D, CornerF32 *c32, Carver *node_cv = nullptr);
+
+// bytes of x, y, z, xd, yd, zd of a domain of `numNode` nodes, as carved
+size_t node_region_bytes(size_t numNode);
 
 // Write the geometry and connectivity arrays of single domain D (tp = 1) on
 // the device (setup.cu), with the values build_domain computes on the

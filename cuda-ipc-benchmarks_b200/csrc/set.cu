@@ -163,7 +163,18 @@ static int create_common(lulesh_set *s, const std::vector<DomPlace> &place, int 
     LCHECK(cudaMalloc(&s->arena, total));
     if (mixed) LCHECK(cudaMalloc(&s->dcorner32, sizeof(CornerF32) * s->ndom));
 
-    Carver cv{static_cast<char *>(s->arena)};
+    // subdomain sets: every domain's x..zd side by side at the start of the
+    // arena (the node region), so one L2 window can cover them all; the
+    // arena's size is the same, the rest of each domain follows
+    size_t node_region = 0;
+    if (!s->unstructured && s->tp > 1)
+        for (int d = 0; d < s->ndom; ++d) {
+            const size_t e1 = (size_t)s->jobs[place[d].job].nx + 1;
+            node_region += node_region_bytes(e1 * e1 * e1);
+        }
+    Carver ncv{static_cast<char *>(s->arena)};
+    Carver cv{static_cast<char *>(s->arena) + node_region};
+    s->node_region_bytes = node_region;
     s->hdoms.resize(s->ndom);
     s->dom_rank.resize(s->ndom);
     s->dom_job.resize(s->ndom);
@@ -186,7 +197,8 @@ static int create_common(lulesh_set *s, const std::vector<DomPlace> &place, int 
                          j.cost,
                          /*global_mass=*/pl.tp > 1 && (s->flags & LULESH_FLAG_HOST_SETUP));
         DomDev D{};
-        int su = upload_domain(h, pl.job, commd[d], mixed, cv, s->stream, &D, &hc32[d]);
+        int su = upload_domain(h, pl.job, commd[d], mixed, cv, s->stream, &D, &hc32[d],
+                               node_region ? &ncv : nullptr);
         if (su != LULESH_OK) return su;
         s->hdoms[d] = D;
         s->dom_rank[d] = pl.rank;
@@ -299,12 +311,13 @@ int enqueue_cycle(lulesh_set *s)
 // A single domain keeps its node coordinate and velocity arrays (x..zd,
 // ~50 MB at -s 100, contiguous in the arena) persisting in L2: force reads
 // them, nodal reads and writes them, kinematics reads them again, every
-// cycle.  The access-policy window is a stream attribute, captured into
-// the cycle graph's kernel nodes.  Only when those arrays take at most half
-// of the L2: measured on B200, the window takes -s 100 (49.5 MB) from 332.0
-// to 327.4 us per cycle, but -s 120 (85 MB) from 559.7 to 610.2 us (566.1
-// with the persisting lines capped at 48 MB); the results are the same.
-// Batches and subdomain sets do not use it.
+// cycle; so does a subdomain set, whose domains' x..zd share the node
+// region at the start of the arena.  The access-policy window is a stream
+// attribute, captured into the cycle graph's kernel nodes.  Only when
+// those arrays take at most half of the L2: measured on B200, the window
+// takes -s 100 (49.5 MB) from 332.0 to 327.4 us per cycle, but -s 120
+// (85 MB) from 559.7 to 610.2 us (566.1 with the persisting lines capped at
+// 48 MB); the results are the same.  Batches do not use it.
 // 0 leaves every set's stream without an access-policy window
 #ifndef LULESH_L2_WINDOW
 #define LULESH_L2_WINDOW 1
@@ -350,7 +363,8 @@ static int l2_node_window_on_device(lulesh_set *s);
 // current for the call, whatever device the calling thread has
 static int l2_node_window(lulesh_set *s)
 {
-    if (!LULESH_L2_WINDOW || s->ndom != 1 || s->l2_window) return LULESH_OK;
+    if (!LULESH_L2_WINDOW || (s->ndom != 1 && !s->node_region_bytes) || s->l2_window)
+        return LULESH_OK;
     int prev = -1;
     LCHECK(cudaGetDevice(&prev));
     if (prev != s->device) LCHECK(cudaSetDevice(s->device));
@@ -361,11 +375,14 @@ static int l2_node_window(lulesh_set *s)
 
 static int l2_node_window_on_device(lulesh_set *s)
 {
-    if (!LULESH_L2_WINDOW || s->ndom != 1 || s->device < 0 || s->device >= 64) return LULESH_OK;
-    if (s->l2_window) return LULESH_OK;  // already on the stream (graph rebuilt)
+    if (s->device < 0 || s->device >= 64) return LULESH_OK;
     const DomDev &D = s->hdoms[0];
     const char *lo = reinterpret_cast<const char *>(D.x);
     const char *hi = reinterpret_cast<const char *>(D.zd + D.numNode);
+    if (s->node_region_bytes) {  // every domain's x..zd: the node region
+        lo = static_cast<const char *>(s->arena);
+        hi = lo + s->node_region_bytes;
+    }
     int maxwin = 0, maxpersist = 0, l2 = 0;
     LCHECK(cudaDeviceGetAttribute(&maxwin, cudaDevAttrMaxAccessPolicyWindowSize, s->device));
     LCHECK(cudaDeviceGetAttribute(&maxpersist, cudaDevAttrMaxPersistingL2CacheSize, s->device));

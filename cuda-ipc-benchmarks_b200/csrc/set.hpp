@@ -69,9 +69,11 @@ struct lulesh_set {
     // launch the cycle kernels with programmatic dependent launch
     bool pdl = LULESH_PDL != 0;
 
-    // the arena
+    // the arena; subdomain sets start it with the node region (every
+    // domain's x..zd, node_region_bytes), single domains carve in place
     void *arena = nullptr;
     size_t arena_bytes = 0;
+    size_t node_region_bytes = 0;
 
     // captured cycle, and a graph of graph_cycles consecutive cycles
     cudaGraph_t graph = nullptr;
