@@ -206,6 +206,35 @@ __device__ __forceinline__ void gather_corners(const DomDev *doms, const DomDev 
 {
     const int nx = D.nx;
     fx = fy = fz = 0.0;
+    if (D.tp > 1) {
+        // subdomains: the source domain of each corner first (this one or
+        // a neighbour), then one load path that the warp shares
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int ex = px - kCX[j], ey = py - kCY[j], ez = pz - kCZ[j];
+            const int sx = (ex < 0) ? -1 : (ex >= nx ? 1 : 0);
+            const int sy = (ey < 0) ? -1 : (ey >= nx ? 1 : 0);
+            const int sz = (ez < 0) ? -1 : (ez >= nx ? 1 : 0);
+            const DomDev *S = &D;
+            bool use = (sx | sy | sz) == 0;
+            if (!use) {
+                const int nb = D.nbr[(sx + 1) + 3 * (sy + 1) + 9 * (sz + 1)];
+                if (nb >= 0) {
+                    S = &doms[nb];
+                    use = true;
+                }
+            }
+            if (use) {
+                const int lx = ex - sx * nx, ly = ey - sy * nx, lz = ez - sz * nx;
+                const int idx = chk_index(j * S->Ep + (lz * nx + ly) * nx + lx, 8LL * S->Ep, T,
+                                          kChkCorner);
+                fx += ld_corner(S->fx_elem + idx);
+                fy += ld_corner(S->fy_elem + idx);
+                fz += ld_corner(S->fz_elem + idx);
+            }
+        }
+        return;
+    }
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         const int ex = px - kCX[j], ey = py - kCY[j], ez = pz - kCZ[j];
@@ -217,20 +246,6 @@ __device__ __forceinline__ void gather_corners(const DomDev *doms, const DomDev 
             fx += ld_corner(D.fx_elem + idx);
             fy += ld_corner(D.fy_elem + idx);
             fz += ld_corner(D.fz_elem + idx);
-        } else if (D.tp > 1) {
-            const int sx = (ex < 0) ? -1 : (ex >= nx ? 1 : 0);
-            const int sy = (ey < 0) ? -1 : (ey >= nx ? 1 : 0);
-            const int sz = (ez < 0) ? -1 : (ez >= nx ? 1 : 0);
-            const int nb = D.nbr[(sx + 1) + 3 * (sy + 1) + 9 * (sz + 1)];
-            if (nb >= 0) {
-                const DomDev &N = doms[nb];
-                const int lx = ex - sx * nx, ly = ey - sy * nx, lz = ez - sz * nx;
-                const int idx = chk_index(j * N.Ep + (lz * nx + ly) * nx + lx, 8LL * N.Ep,
-                                          T, kChkCorner);
-                fx += ld_corner(N.fx_elem + idx);
-                fy += ld_corner(N.fy_elem + idx);
-                fz += ld_corner(N.fz_elem + idx);
-            }
         }
     }
 }
