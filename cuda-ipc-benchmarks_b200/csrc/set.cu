@@ -12,6 +12,11 @@
 #include "halo_plan.hpp"
 #include "set.hpp"
 
+// 0: the fused subdomain cycle leaves out the PosVel sync kernel
+#ifndef LULESH_FUSED_POSVEL_SYNC
+#define LULESH_FUSED_POSVEL_SYNC 1
+#endif
+
 namespace lulesh {
 
 static thread_local std::string g_last_error;
@@ -295,7 +300,7 @@ int enqueue_cycle(lulesh_set *s)
     else
         launch_nodal(s->args(s->node_blocks), s->n_node_blocks, s->P, st, s->nb,
                          s->unstructured);
-    if (s->tp > 1 && s->n_sync_blocks > 0)
+    if (LULESH_FUSED_POSVEL_SYNC && s->tp > 1 && s->n_sync_blocks > 0)
         launch_posvel_sync(s->args(s->sync_blocks), s->n_sync_blocks, st);
     if (mixed)
         launch_kinematics_mixed(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st);
@@ -944,7 +949,7 @@ int lulesh_profile_phases(lulesh_set *s, int ncycles, double *ms_out, int *nphas
             launch_nodal(s->args(s->node_blocks), s->n_node_blocks, s->P, st, s->nb,
                          s->unstructured);
         LCHECK(cudaEventRecord(ev[3], st));
-        if (s->tp > 1 && s->n_sync_blocks > 0)
+        if (LULESH_FUSED_POSVEL_SYNC && s->tp > 1 && s->n_sync_blocks > 0)
             launch_posvel_sync(s->args(s->sync_blocks), s->n_sync_blocks, st);
         LCHECK(cudaEventRecord(ev[4], st));
         if (mixed)
