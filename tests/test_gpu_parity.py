@@ -126,27 +126,34 @@ def test_region_flags_do_not_change_results(lulesh):
     assert np.array_equal(res[0], res[1]) and np.array_equal(res[0], res[2])
 
 
-@pytest.mark.parametrize("tp,nx", [(2, 6), (2, 9), (3, 4)])
+@pytest.mark.parametrize("tp,nx", [(2, 6), (2, 9), (3, 4), (4, 5)])
 def test_subdomains_bitwise_equal_single_domain(lulesh, tp, nx):
     """tp^3 in-device subdomains of -s nx reproduce the single -s tp*nx
-    domain exactly: corner forces are gathered across subdomain faces in the
-    undecomposed corner order, and nodal mass is summed in global order."""
-    cycles = 30
-    with lulesh.LuleshSet(nx=tp * nx, its=cycles) as single:
+    domain exactly, every node and element field of every subdomain:
+    corner forces are gathered across subdomain faces in the undecomposed
+    corner order and nodal mass is summed in global order, so both copies of
+    a shared node are computed alike and need no PosVel copy."""
+    cycles = 200
+    node = ["x", "y", "z", "xd", "yd", "zd"]
+    elem = ["e", "p", "q", "v", "ss"]
+    G = tp * nx
+    with lulesh.LuleshSet(nx=G, its=cycles) as single:
         assert single.run() == lulesh.OK
-        e_single = single.field("e").reshape(tp * nx, tp * nx, tp * nx)
-        x_single = single.field("x").reshape(tp * nx + 1, tp * nx + 1, tp * nx + 1)
+        ref_n = {f: single.field(f).reshape(G + 1, G + 1, G + 1) for f in node}
+        ref_e = {f: single.field(f).reshape(G, G, G) for f in elem}
     with lulesh.LuleshSet(nx=nx, tp=tp, its=cycles) as sub:
         assert sub.run() == lulesh.OK
         for r in range(tp ** 3):
             c, w, p = r % tp, (r // tp) % tp, r // (tp * tp)
-            e = sub.field("e", domain=r).reshape(nx, nx, nx)
-            ref = e_single[p * nx:(p + 1) * nx, w * nx:(w + 1) * nx, c * nx:(c + 1) * nx]
-            assert np.array_equal(e, ref), f"rank {r}"
-            x = sub.field("x", domain=r).reshape(nx + 1, nx + 1, nx + 1)
-            refx = x_single[p * nx:(p + 1) * nx + 1, w * nx:(w + 1) * nx + 1,
-                            c * nx:(c + 1) * nx + 1]
-            assert np.array_equal(x, refx), f"rank {r}"
+            for f in elem:
+                got = sub.field(f, domain=r)[:nx ** 3].reshape(nx, nx, nx)
+                want = ref_e[f][p * nx:(p + 1) * nx, w * nx:(w + 1) * nx, c * nx:(c + 1) * nx]
+                assert np.array_equal(got, want), (r, f)
+            for f in node:
+                got = sub.field(f, domain=r).reshape(nx + 1, nx + 1, nx + 1)
+                want = ref_n[f][p * nx:(p + 1) * nx + 1, w * nx:(w + 1) * nx + 1,
+                                c * nx:(c + 1) * nx + 1]
+                assert np.array_equal(got, want), (r, f)
 
 
 def test_subdomains_staged_comm_matches(lulesh):
