@@ -16,10 +16,10 @@
 //                   CalcTimeConstraintsForElems (lulesh.cu:3554-3725,
 //                   3988-4097, 4216-4403) fused; the dt minimum is reduced
 //                   with warp shuffles and one 64-bit atomicMin per block
-// Subdomain sets add the MonoQ ghost kernel; the parts of a multi-GPU
-// problem also run the PosVel sync kernel after their POSVEL messages (a
-// set holding every subdomain computes both copies of a shared node alike
-// and leaves it out).
+// Subdomain sets add the MonoQ ghost kernel.  The PosVel sync kernel copies
+// a neighbour's max-side node layer (CommSyncPosVel semantics); a cycle in
+// which every corner of every node is summed in single-domain order does
+// not need it, and the library's own cycles leave it out.
 // Unstructured (lmesh) domains run force, kinematics and EOS with U = true,
 // which reads nodelist, the face links and elemBC from memory instead of
 // computing them from the element index, and k_nodal_u for the nodal step.

@@ -333,11 +333,27 @@ class DirectTransport:
 class Engine:
     """Drives the parts of this process through set-up and cycles.  The
     order is that of LagrangeLeapFrog (lulesh.cu:4438-4452) with each halo
-    exchange where the reference calls its comm backend."""
+    exchange where the reference calls its comm backend.
 
-    def __init__(self, parts, transport):
+    sync_posvel: also exchange the POSVEL messages and copy them into the
+    receivers' max-side node faces (CommSyncPosVel).  Off by default: each
+    part receives every corner force its nodes need (CORNERS) and the
+    global node masses (MASS), sums them in the single-domain order, and so
+    computes the shared nodes exactly as their +side owner does; the copy
+    would write the values already there.  The reference needs it because
+    its ranks add partial sums in their own orders."""
+
+    def __init__(self, parts, transport, sync_posvel: bool = False):
         self.parts = list(parts)
         self.transport = transport
+        self.sync_posvel = sync_posvel
+
+    @property
+    def cycle_kinds(self):
+        """The message kinds exchanged every cycle."""
+        if self.sync_posvel:
+            return CYCLE_KINDS
+        return tuple(k for k in CYCLE_KINDS if k != L.HALO_POSVEL)
 
     def exchange(self, kind: int) -> None:
         if getattr(self.transport, "handles_packing", False):
@@ -364,8 +380,10 @@ class Engine:
         self._phase(L.PHASE_TIME_INCREMENT, L.PHASE_FORCE)
         self.exchange(L.HALO_CORNERS)        # CommSend + CommSBN of the forces
         self._phase(L.PHASE_NODAL)
-        self.exchange(L.HALO_POSVEL)         # CommSyncPosVel
-        self._phase(L.PHASE_POSVEL_SYNC, L.PHASE_KINEMATICS)
+        if self.sync_posvel:
+            self.exchange(L.HALO_POSVEL)     # CommSyncPosVel
+            self._phase(L.PHASE_POSVEL_SYNC)
+        self._phase(L.PHASE_KINEMATICS)
         self.exchange(L.HALO_MONOQ)          # CommMonoQ
         self._phase(L.PHASE_MONOQ_GHOST, L.PHASE_EOS)
         bufs = [p.dt_pack() for p in self.parts]
@@ -381,8 +399,8 @@ class Engine:
         """Kernels one cycle launches on each part (phases, packs, unpacks,
         dt pack/unpack; transport kernels not counted)."""
         p = self.parts[0]
-        n = 7 + 2
-        for k in CYCLE_KINDS:
+        n = (7 if self.sync_posvel else 6) + 2
+        for k in self.cycle_kinds:
             n += sum(1 for b in p.send[k].values() if b.numel())
             n += sum(1 for b in p.recv[k].values() if b.numel())
         return n
@@ -449,7 +467,7 @@ def bench_decomposed(warmup: int, steps: int, dist, transport: str = "nccl",
            "global_nx": nx * tp, "zones_total": (nx * tp) ** 3, "transport": tr.name,
            "energy": energy, "cycle": st["cycle"], "status": st["status"],
            "launches_per_cycle": eng.launches_per_cycle(),
-           "halo_bytes_per_cycle": 8 * part.halo_doubles()}
+           "halo_bytes_per_cycle": 8 * part.halo_doubles(eng.cycle_kinds)}
     part.close()
     return out
 

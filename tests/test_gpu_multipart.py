@@ -28,8 +28,9 @@ def _region(nx, tp, r):
     return ge, gn
 
 
-@pytest.mark.parametrize("nparts", [2, 4, 8])
-def test_parts_on_one_gpu_match_single_domain(lulesh, nparts):
+@pytest.mark.parametrize("nparts,sync_posvel", [(2, False), (4, False), (8, False), (2, True),
+                                                (8, True)])
+def test_parts_on_one_gpu_match_single_domain(lulesh, nparts, sync_posvel):
     torch = pytest.importorskip("torch")
     import distributed as D
 
@@ -37,7 +38,7 @@ def test_parts_on_one_gpu_match_single_domain(lulesh, nparts):
     stream = torch.cuda.Stream()
     with torch.cuda.stream(stream):
         parts = [D.GpuPart(nx, tp, nparts, p, device=0, stream=stream) for p in range(nparts)]
-        eng = D.Engine(parts, D.LocalTransport())
+        eng = D.Engine(parts, D.LocalTransport(), sync_posvel=sync_posvel)
         eng.setup()
         eng.run(cycles)
     torch.cuda.synchronize()
@@ -189,8 +190,8 @@ def test_two_processes_on_one_gpu_match_single_domain(lulesh):
                 assert np.array_equal(f_d[f], ref[f][gn]), (rank, d, f)
 
 
-@pytest.mark.parametrize("nparts", [2, 8])
-def test_direct_transport_parts_on_one_gpu(lulesh, nparts):
+@pytest.mark.parametrize("nparts,sync_posvel", [(2, False), (8, False), (8, True)])
+def test_direct_transport_parts_on_one_gpu(lulesh, nparts, sync_posvel):
     """The direct transport with every part in this process: each put kernel
     stores its message into the receiver's mailbox and raises the flag
     before the receiver's take kernel runs (one stream), so no wait spins.
@@ -202,7 +203,7 @@ def test_direct_transport_parts_on_one_gpu(lulesh, nparts):
     stream = torch.cuda.Stream()
     with torch.cuda.stream(stream):
         parts = [D.GpuPart(nx, tp, nparts, p, device=0, stream=stream) for p in range(nparts)]
-        eng = D.Engine(parts, D.DirectTransport())
+        eng = D.Engine(parts, D.DirectTransport(), sync_posvel=sync_posvel)
         eng.setup()
         eng.run(cycles)
     torch.cuda.synchronize()

@@ -61,11 +61,14 @@ def test_plan_pairs_are_symmetric_in_size():
     assert len(D.plan(nx, 2, 8, 0, 1, D.L.HALO_MONOQ)[0]) == nx * nx * 3
 
 
+@pytest.mark.parametrize("sync_posvel", [False, True])
 @pytest.mark.parametrize("nparts", [1, 2, 4, 8])
-def test_local_parts_match_single_domain(nparts):
+def test_local_parts_match_single_domain(nparts, sync_posvel):
+    """With or without the POSVEL exchange (the engine leaves it out by
+    default: each part computes its shared nodes as their owner does)."""
     nx, cycles = 4, 25
     parts = [OraclePart(nx, 2, nparts, p) for p in range(nparts)]
-    eng = D.Engine(parts, D.LocalTransport())
+    eng = D.Engine(parts, D.LocalTransport(), sync_posvel=sync_posvel)
     eng.setup()
     eng.run(cycles)
     single = _single(2 * nx, cycles)
