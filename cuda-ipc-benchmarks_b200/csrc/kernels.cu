@@ -603,6 +603,43 @@ __device__ __forceinline__ double mono_limiter(const double *delv, int i, int bc
     return phi;
 }
 
+// mono_limiter with the minus and plus neighbours read from their own
+// arrays (dm[lm], dp[lp]): a comm face's neighbour element is then read in
+// the neighbouring subdomain instead of from this subdomain's ghost copy.
+__device__ __forceinline__ double mono_limiter_split(const double *delv, const double *dm,
+                                                     const double *dp, int i, int bc,
+                                                     int mmask, int msymm, int mfree,
+                                                     int pmask, int psymm, int pfree, int lm,
+                                                     int lp, double mult, double maxslope,
+                                                     double ptiny, int nm, int np, TimeCtl *T)
+{
+    const double norm = 1. / (delv[i] + ptiny);
+    double delvm, delvp;
+    const int mb = bc & mmask, pb = bc & pmask;
+    if (mb == msymm)
+        delvm = delv[i];
+    else if (mb == mfree)
+        delvm = 0.0;
+    else
+        delvm = dm[chk_index(lm, nm, T, kChkLink)];
+    if (pb == psymm)
+        delvp = delv[i];
+    else if (pb == pfree)
+        delvp = 0.0;
+    else
+        delvp = dp[chk_index(lp, np, T, kChkLink)];
+    delvm = delvm * norm;
+    delvp = delvp * norm;
+    double phi = .5 * (delvm + delvp);
+    delvm *= mult;
+    delvp *= mult;
+    if (delvm < phi) phi = delvm;
+    if (delvp < phi) phi = delvp;
+    if (phi < 0.) phi = 0.;
+    if (phi > maxslope) phi = maxslope;
+    return phi;
+}
+
 // CalcPressureForElems_device, lulesh.cu:3764-3791
 __device__ __forceinline__ void calc_pressure(double &p_new, double &bvc, double &pbvc,
                                               double &e_old, double &compression,
@@ -685,7 +722,9 @@ __device__ __forceinline__ double warp_min(double v)
     return v;
 }
 
-template <int BS, bool U = false>
+// SUB: a subdomain set's fused cycle, which reads a comm face's neighbour
+// element in the neighbouring subdomain (no MonoQ ghost copy)
+template <int BS, bool U = false, bool SUB = false>
 __global__ void __launch_bounds__(BS, min_blocks(kEosMinBlocks, BS)) k_eos(SetArgs a, Params P)
 {
     pdl_enter();
@@ -722,15 +761,58 @@ __global__ void __launch_bounds__(BS, min_blocks(kEosMinBlocks, BS)) k_eos(SetAr
             elem_face_links(D, zidx, bcMask, lxm, lxp, lem, lep, lzm, lzp);
         }
         const double mult = P.monoq_limiter_mult, maxs = P.monoq_max_slope;
-        const double phixi =
-            mono_limiter(D.delv_xi, zidx, bcMask, XI_M, XI_M_SYMM, XI_M_FREE, XI_P, XI_P_SYMM,
-                         XI_P_FREE, lxm, lxp, mult, maxs, ptiny, D.allElem, &T);
-        const double phieta =
-            mono_limiter(D.delv_eta, zidx, bcMask, ETA_M, ETA_M_SYMM, ETA_M_FREE, ETA_P,
-                         ETA_P_SYMM, ETA_P_FREE, lem, lep, mult, maxs, ptiny, D.allElem, &T);
-        const double phizeta =
-            mono_limiter(D.delv_zeta, zidx, bcMask, ZETA_M, ZETA_M_SYMM, ZETA_M_FREE, ZETA_P,
-                         ZETA_P_SYMM, ZETA_P_FREE, lzm, lzp, mult, maxs, ptiny, D.allElem, &T);
+        double phixi, phieta, phizeta;
+        if (SUB) {
+            // comm faces: the mirrored element of the neighbour's opposite
+            // face layer, where k_monoq_ghost would copy it from
+            const int nx = D.nx;
+            const int ix = zidx % nx, t = zidx / nx, iy = t % nx, iz = t / nx;
+            const DomDev *sxm = &D, *sxp = &D, *sem = &D, *sep = &D, *szm = &D, *szp = &D;
+            if (bcMask & XI_M_COMM) {
+                sxm = &a.doms[D.nbr[0 + 3 + 9]];
+                lxm = (iz * nx + iy) * nx + (nx - 1);
+            }
+            if (bcMask & XI_P_COMM) {
+                sxp = &a.doms[D.nbr[2 + 3 + 9]];
+                lxp = (iz * nx + iy) * nx;
+            }
+            if (bcMask & ETA_M_COMM) {
+                sem = &a.doms[D.nbr[1 + 0 + 9]];
+                lem = (iz * nx + (nx - 1)) * nx + ix;
+            }
+            if (bcMask & ETA_P_COMM) {
+                sep = &a.doms[D.nbr[1 + 6 + 9]];
+                lep = (iz * nx) * nx + ix;
+            }
+            if (bcMask & ZETA_M_COMM) {
+                szm = &a.doms[D.nbr[1 + 3 + 0]];
+                lzm = ((nx - 1) * nx + iy) * nx + ix;
+            }
+            if (bcMask & ZETA_P_COMM) {
+                szp = &a.doms[D.nbr[1 + 3 + 18]];
+                lzp = iy * nx + ix;
+            }
+            phixi = mono_limiter_split(D.delv_xi, sxm->delv_xi, sxp->delv_xi, zidx, bcMask, XI_M,
+                                       XI_M_SYMM, XI_M_FREE, XI_P, XI_P_SYMM, XI_P_FREE, lxm, lxp,
+                                       mult, maxs, ptiny, sxm->allElem, sxp->allElem, &T);
+            phieta = mono_limiter_split(D.delv_eta, sem->delv_eta, sep->delv_eta, zidx, bcMask,
+                                        ETA_M, ETA_M_SYMM, ETA_M_FREE, ETA_P, ETA_P_SYMM,
+                                        ETA_P_FREE, lem, lep, mult, maxs, ptiny, sem->allElem,
+                                        sep->allElem, &T);
+            phizeta = mono_limiter_split(D.delv_zeta, szm->delv_zeta, szp->delv_zeta, zidx,
+                                         bcMask, ZETA_M, ZETA_M_SYMM, ZETA_M_FREE, ZETA_P,
+                                         ZETA_P_SYMM, ZETA_P_FREE, lzm, lzp, mult, maxs, ptiny,
+                                         szm->allElem, szp->allElem, &T);
+        } else {
+            phixi = mono_limiter(D.delv_xi, zidx, bcMask, XI_M, XI_M_SYMM, XI_M_FREE, XI_P,
+                                 XI_P_SYMM, XI_P_FREE, lxm, lxp, mult, maxs, ptiny, D.allElem, &T);
+            phieta = mono_limiter(D.delv_eta, zidx, bcMask, ETA_M, ETA_M_SYMM, ETA_M_FREE, ETA_P,
+                                  ETA_P_SYMM, ETA_P_FREE, lem, lep, mult, maxs, ptiny, D.allElem,
+                                  &T);
+            phizeta = mono_limiter(D.delv_zeta, zidx, bcMask, ZETA_M, ZETA_M_SYMM, ZETA_M_FREE,
+                                   ZETA_P, ZETA_P_SYMM, ZETA_P_FREE, lzm, lzp, mult, maxs, ptiny,
+                                   D.allElem, &T);
+        }
         const double vdov_z = D.vdov[zidx];
         const double vnew_z = D.vnew[zidx];
         double qlin, qquad;
@@ -868,10 +950,15 @@ __global__ void __launch_bounds__(BS, min_blocks(kEosMinBlocks, BS)) k_eos(SetAr
     }
 }
 
-void launch_eos(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs, bool u)
+void launch_eos(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs, bool u,
+                bool sub)
 {
     if (u) {
         launch_k(k_eos<kElemBlock, true>, nblocks, kElemBlock, s, a.pdl != 0, a, P);
+        return;
+    }
+    if (sub) {  // subdomain sets take 128-element blocks only
+        launch_k(k_eos<kElemBlock, false, true>, nblocks, kElemBlock, s, a.pdl != 0, a, P);
         return;
     }
     switch (bs) {

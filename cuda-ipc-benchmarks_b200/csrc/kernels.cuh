@@ -152,8 +152,10 @@ void launch_nodal_gather_local(const SetArgs &a, int nblocks, cudaStream_t s);
 void launch_nodal_update(const SetArgs &a, int nblocks, Params P, cudaStream_t s);
 void launch_kinematics(const SetArgs &a, int nblocks, Params P, cudaStream_t s,
                        int bs = kElemBlock, bool u = false);
+// sub: a subdomain set's fused cycle, comm-face neighbours read in the
+// neighbouring subdomain (k_monoq_ghost not needed)
 void launch_eos(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs = kElemBlock,
-                bool u = false);
+                bool u = false, bool sub = false);
 // fused halo kernels of a subdomain set (direct reads of neighbour memory)
 void launch_posvel_sync(const SetArgs &a, int nblocks, cudaStream_t s);
 void launch_monoq_ghost(const SetArgs &a, int nblocks, cudaStream_t s);

@@ -27,6 +27,13 @@
 #ifndef LULESH_FUSED_POSVEL_SYNC
 #define LULESH_FUSED_POSVEL_SYNC 0
 #endif
+// The fused subdomain cycle's EOS reads a comm face's neighbour element in
+// the neighbouring subdomain (k_eos<..., SUB>), the value k_monoq_ghost
+// would copy into this subdomain's ghost face (CommMonoQ semantics,
+// lulesh-comms-gpu.cu:1665-1806).  1 copies the ghost faces and reads them.
+#ifndef LULESH_FUSED_MONOQ_GHOST
+#define LULESH_FUSED_MONOQ_GHOST 0
+#endif
 
 namespace lulesh {
 
@@ -318,9 +325,10 @@ int enqueue_cycle(lulesh_set *s)
     else
         launch_kinematics(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb,
                               s->unstructured);
-    if (s->tp > 1 && s->n_ghost_blocks > 0)
+    if (LULESH_FUSED_MONOQ_GHOST && s->tp > 1 && s->n_ghost_blocks > 0)
         launch_monoq_ghost(s->args(s->ghost_blocks), s->n_ghost_blocks, st);
-    launch_eos(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb, s->unstructured);
+    launch_eos(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb, s->unstructured,
+               !LULESH_FUSED_MONOQ_GHOST && s->tp > 1);
     return cuda_status(cudaGetLastError(), "cycle launch");
 }
 
@@ -969,10 +977,11 @@ int lulesh_profile_phases(lulesh_set *s, int ncycles, double *ms_out, int *nphas
             launch_kinematics(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb,
                               s->unstructured);
         LCHECK(cudaEventRecord(ev[5], st));
-        if (s->tp > 1 && s->n_ghost_blocks > 0)
+        if (LULESH_FUSED_MONOQ_GHOST && s->tp > 1 && s->n_ghost_blocks > 0)
             launch_monoq_ghost(s->args(s->ghost_blocks), s->n_ghost_blocks, st);
         LCHECK(cudaEventRecord(ev[6], st));
-        launch_eos(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb, s->unstructured);
+        launch_eos(s->args(s->elem_blocks), s->n_elem_blocks, s->P, st, s->eb, s->unstructured,
+                   !LULESH_FUSED_MONOQ_GHOST && s->tp > 1);
         LCHECK(cudaEventRecord(ev[7], st));
         LCHECK(cudaEventSynchronize(ev[7]));
         for (int k = 0; k < np; ++k) {
