@@ -16,10 +16,12 @@
 //                   CalcTimeConstraintsForElems (lulesh.cu:3554-3725,
 //                   3988-4097, 4216-4403) fused; the dt minimum is reduced
 //                   with warp shuffles and one 64-bit atomicMin per block
-// Subdomain sets add the MonoQ ghost kernel.  The PosVel sync kernel copies
-// a neighbour's max-side node layer (CommSyncPosVel semantics); a cycle in
-// which every corner of every node is summed in single-domain order does
-// not need it, and the library's own cycles leave it out.
+// Two halo kernels follow CommSyncPosVel and CommMonoQ: the PosVel sync
+// copies a neighbour's max-side node layer, the MonoQ ghost kernel its
+// boundary element layer of delv_*.  A subdomain set's fused cycle needs
+// neither (every corner of every node is summed in single-domain order, and
+// k_eos<..., SUB> reads comm-face neighbours in place); the parts of a
+// multi-GPU problem use the MonoQ ghost kernel after their MONOQ messages.
 // Unstructured (lmesh) domains run force, kinematics and EOS with U = true,
 // which reads nodelist, the face links and elemBC from memory instead of
 // computing them from the element index, and k_nodal_u for the nodal step.
