@@ -438,9 +438,15 @@ int lulesh_part_phase(lulesh_set *s, int phase)
             launch_kinematics(ae, s->n_elem_blocks, s->P, st, s->eb, false);
             break;
         case LULESH_PHASE_MONOQ_GHOST:
-            if (s->tp > 1 && s->n_ghost_blocks > 0) launch_monoq_ghost(ag, s->n_ghost_blocks, st);
+            // nothing to copy unless the EOS reads ghost faces (the proxies
+            // hold the neighbours' layers after the MONOQ messages)
+            if (LULESH_FUSED_MONOQ_GHOST && s->tp > 1 && s->n_ghost_blocks > 0)
+                launch_monoq_ghost(ag, s->n_ghost_blocks, st);
             break;
-        case LULESH_PHASE_EOS: launch_eos(ae, s->n_elem_blocks, s->P, st, s->eb, false); break;
+        case LULESH_PHASE_EOS:
+            launch_eos(ae, s->n_elem_blocks, s->P, st, s->eb, false,
+                       !LULESH_FUSED_MONOQ_GHOST && s->tp > 1);
+            break;
         default: set_error("lulesh_part_phase: unknown phase"); return LULESH_INVALID_ARG;
     }
     return cuda_status(cudaGetLastError(), "part phase");

@@ -27,13 +27,6 @@
 #ifndef LULESH_FUSED_POSVEL_SYNC
 #define LULESH_FUSED_POSVEL_SYNC 0
 #endif
-// The fused subdomain cycle's EOS reads a comm face's neighbour element in
-// the neighbouring subdomain (k_eos<..., SUB>), the value k_monoq_ghost
-// would copy into this subdomain's ghost face (CommMonoQ semantics,
-// lulesh-comms-gpu.cu:1665-1806).  1 copies the ghost faces and reads them.
-#ifndef LULESH_FUSED_MONOQ_GHOST
-#define LULESH_FUSED_MONOQ_GHOST 0
-#endif
 
 namespace lulesh {
 

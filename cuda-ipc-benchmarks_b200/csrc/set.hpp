@@ -18,6 +18,15 @@
 #define LULESH_NODAL_REVERSE 1
 #endif
 
+// The EOS of a subdomain set's fused cycle, and of a part of a multi-GPU
+// problem, reads a comm face's neighbour element in the neighbouring
+// subdomain or its proxy (k_eos<..., SUB>): the value k_monoq_ghost would
+// copy into this subdomain's ghost face (CommMonoQ semantics,
+// lulesh-comms-gpu.cu:1665-1806).  1 copies the ghost faces and reads them.
+#ifndef LULESH_FUSED_MONOQ_GHOST
+#define LULESH_FUSED_MONOQ_GHOST 0
+#endif
+
 // 0 launches every cycle kernel with plain stream order
 #ifndef LULESH_PDL
 #define LULESH_PDL 1

@@ -480,9 +480,12 @@ int lulesh_halo_pack(lulesh_set *set, int kind, int peer, double *dev_buf);
 int lulesh_halo_unpack(lulesh_set *set, int kind, int peer, const double *dev_buf);
 
 /* One phase of the cycle, enqueued on the set's stream.  A cycle of a part
- * is: TIME_INCREMENT, FORCE, exchange CORNERS, NODAL, exchange POSVEL,
- * POSVEL_SYNC, KINEMATICS, exchange MONOQ, MONOQ_GHOST, EOS, then the dt
- * reduction below. */
+ * is: TIME_INCREMENT, FORCE, exchange CORNERS, NODAL, [exchange POSVEL,
+ * POSVEL_SYNC,] KINEMATICS, exchange MONOQ, MONOQ_GHOST, EOS, then the dt
+ * reduction below.  The POSVEL exchange and its sync may be left out (the
+ * part computes its shared nodes exactly as their owner does).
+ * MONOQ_GHOST enqueues nothing in this build: the EOS reads the
+ * neighbours' delv layers in the proxies the MONOQ messages filled. */
 #define LULESH_PHASE_TIME_INCREMENT 0
 #define LULESH_PHASE_FORCE 1
 #define LULESH_PHASE_NODAL 2
