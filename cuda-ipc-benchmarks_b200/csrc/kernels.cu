@@ -20,8 +20,8 @@
 // copies a neighbour's max-side node layer, the MonoQ ghost kernel its
 // boundary element layer of delv_*.  A subdomain set's fused cycle needs
 // neither (every corner of every node is summed in single-domain order, and
-// k_eos<..., SUB> reads comm-face neighbours in place); the parts of a
-// multi-GPU problem use the MonoQ ghost kernel after their MONOQ messages.
+// k_eos<..., SUB> reads comm-face neighbours in place), and the parts of a
+// multi-GPU problem read their proxies in place after the MONOQ messages.
 // Unstructured (lmesh) domains run force, kinematics and EOS with U = true,
 // which reads nodelist, the face links and elemBC from memory instead of
 // computing them from the element index, and k_nodal_u for the nodal step.
