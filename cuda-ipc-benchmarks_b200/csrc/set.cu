@@ -22,8 +22,9 @@
 // on the same values and stay equal bit for bit (checked against the single
 // domain, every field, 2^3, 3^3 and 4^3 subdomains, up to 400 cycles).
 // Leaving the copy out takes 2x2x2 of -s 50 from 349.5 to 343.9 us per
-// cycle.  1 puts the k_posvel_sync launch back in the fused cycle; the
-// staged Comm* path and the parts of a multi-GPU problem always exchange.
+// cycle.  1 puts the k_posvel_sync launch back in the fused cycle.  The
+// staged Comm* path keeps the reference's exchange; the parts of a
+// multi-GPU problem exchange POSVEL only when their driver asks for it.
 #ifndef LULESH_FUSED_POSVEL_SYNC
 #define LULESH_FUSED_POSVEL_SYNC 0
 #endif
