@@ -35,6 +35,13 @@
 
 namespace lulesh {
 
+// elements per block of the served cycle's element kernels (64, 128 or 256)
+#ifndef LULESH_SERVER_ELEM_BLOCK
+#define LULESH_SERVER_ELEM_BLOCK 128
+#endif
+constexpr int kServerElemBlock = LULESH_SERVER_ELEM_BLOCK;
+static_assert(valid_elem_block(kServerElemBlock), "64, 128 or 256 elements per block");
+
 struct SJob {
     long long id = 0;
     lulesh_job job{};
@@ -150,7 +157,7 @@ static int rebuild(lulesh_server *s)
         const DomDev &D = order[d]->dom;
         hd.push_back(D);
         for (int i = 0; i < D.numNode; i += kNodeBlock) nb.push_back(make_int2((int)d, i));
-        for (int i = 0; i < D.numElem; i += kElemBlock) eb.push_back(make_int2((int)d, i));
+        for (int i = 0; i < D.numElem; i += kServerElemBlock) eb.push_back(make_int2((int)d, i));
     }
     // the nodal kernel walks last to first, as for sets (build_tables)
     if (LULESH_NODAL_REVERSE) std::reverse(nb.begin(), nb.end());
@@ -194,10 +201,10 @@ static int rebuild(lulesh_server *s)
     } else {
         SCHECK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
         launch_time_increment(s->dtc, s->cfg.max_jobs, s->P, s->stream, LULESH_PDL != 0);
-        launch_force(s->args(s->elem_b), s->n_elem, s->P, s->stream);
+        launch_force(s->args(s->elem_b), s->n_elem, s->P, s->stream, kServerElemBlock);
         launch_nodal(s->args(s->node_b), s->n_node, s->P, s->stream);
-        launch_kinematics(s->args(s->elem_b), s->n_elem, s->P, s->stream);
-        launch_eos(s->args(s->elem_b), s->n_elem, s->P, s->stream);
+        launch_kinematics(s->args(s->elem_b), s->n_elem, s->P, s->stream, kServerElemBlock);
+        launch_eos(s->args(s->elem_b), s->n_elem, s->P, s->stream, kServerElemBlock);
         cudaGraph_t g = nullptr;
         SCHECK(cudaStreamEndCapture(s->stream, &g));
         // same five kernels every time, only their grids and tables change:
