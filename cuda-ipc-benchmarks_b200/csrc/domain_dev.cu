@@ -178,11 +178,12 @@ int upload_domain(const HostDomain &h, int tc, long comm_doubles, bool mixed, Ca
     if (z.comm) DCHECK(cudaMemsetAsync(D.commRecv, 0, 8 * z.comm, st));
     int su;
     if (h.device_geometry) {
-        // single domain: geometry on the device, regions from the host
+        // single domain: geometry and the per-element region arrays on the
+        // device, the region tables from the host
         if ((su = setup_geometry_on_device(D, h.einit, st)) != LULESH_OK) return su;
-        const std::vector<int> *rv[] = {&h.regNumList, &h.regElemlist, &h.regCSR,
-                                        &h.regReps,    &h.regSorted,   &h.eosOrder};
-        int *rp[] = {D.regNumList, D.regElemlist, D.regCSR, D.regReps, D.regSorted, D.eosOrder};
+        if ((su = setup_regions_on_device(D, h.regionRuns, st)) != LULESH_OK) return su;
+        const std::vector<int> *rv[] = {&h.regCSR, &h.regReps, &h.regSorted};
+        int *rp[] = {D.regCSR, D.regReps, D.regSorted};
         for (size_t k = 0; k < sizeof(rp) / sizeof(rp[0]); ++k)
             if ((su = upload(rp[k], *rv[k], st)) != LULESH_OK) return su;
         DCHECK(cudaStreamSynchronize(st));

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstddef>
+#include <vector>
 
 #include "host_setup.hpp"
 #include "lulesh_b200.h"
@@ -55,6 +56,13 @@ size_t node_region_bytes(size_t numNode);
 // the device (setup.cu), with the values build_domain computes on the
 // host; e[0] = einit.  Asynchronous on `st`.
 int setup_geometry_on_device(const DomDev &D, double einit, cudaStream_t st);
+
+// Write regNumList, regElemlist and eosOrder of single domain D from its
+// region runs (region_runs.hpp), staging the runs in D.fx_elem and zeroing
+// them there again afterwards.  Asynchronous on `st`: `runs` must live until
+// the stream has passed the upload.
+int setup_regions_on_device(const DomDev &D, const std::vector<RegionRun> &runs,
+                            cudaStream_t st);
 
 // The time state of a job before its first cycle (lulesh.cu:1120-1132).
 TimeCtl initial_timectl(double deltatime, int its_cap);

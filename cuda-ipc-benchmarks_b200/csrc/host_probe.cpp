@@ -31,7 +31,8 @@ static long copy_field(const lulesh::HostDomain &d, const char *name, void *out,
                 {"regElemSize", &d.regElemSize}, {"regCSR", &d.regCSR},
                 {"regReps", &d.regReps}, {"regNumList", &d.regNumList},
                 {"regElemlist", &d.regElemlist}, {"regSorted", &d.regSorted},
-                {"nodeBC", &d.nodeBC}, {"nodeCornerEll", &d.nodeCornerEll}};
+                {"nodeBC", &d.nodeBC}, {"nodeCornerEll", &d.nodeCornerEll},
+                {"eosOrder", &d.eosOrder}};
     struct R {
         const char *n;
         const std::vector<double> *v;
@@ -57,6 +58,14 @@ static long copy_field(const lulesh::HostDomain &d, const char *name, void *out,
         if (out && cap >= 1) *(int *)out = d.octantCorner;
         return 1;
     }
+    // the EOS rep classes: end position and rep count of each
+    const int *cls = !std::strcmp(name, "eosClassEnd")   ? d.eosClassEnd
+                     : !std::strcmp(name, "eosClassRep") ? d.eosClassRep
+                                                         : nullptr;
+    if (cls) {
+        if (out && cap >= d.eosNumClass) std::memcpy(out, cls, sizeof(int) * d.eosNumClass);
+        return d.eosNumClass;
+    }
     return -1;
 }
 
@@ -68,6 +77,31 @@ long lulesh_host_domain_field(int nx, int tp, int col, int row, int plane, int r
     lulesh::HostDomain d;
     lulesh::build_domain(d, nx, tp, col, row, plane, rank, numReg, balance, cost,
                          global_mass != 0);
+    return copy_field(d, name, out, cap);
+}
+
+// The light single-domain builder (build_domain_light: the region sets as
+// runs), with regNumList, regElemlist and eosOrder then written from the
+// runs on the host by expand_region_element, the function the device
+// set-up kernel runs per element; "nruns" gives the number of runs.  Copies
+// the named array as copy_field does.
+long lulesh_host_light_field(int nx, int numReg, int balance, int cost, const char *name,
+                             void *out, long cap)
+{
+    lulesh::HostDomain d;
+    lulesh::build_domain_light(d, nx, numReg, balance, cost);
+    if (!std::strcmp(name, "nruns")) {
+        if (out && cap >= 1) *(long *)out = (long)d.regionRuns.size();
+        return 1;
+    }
+    const int E = d.numElem;
+    d.regNumList.assign(E, -1);
+    d.regElemlist.assign(E, -1);
+    d.eosOrder.assign(E, -1);
+    for (int i = 0; i < E; ++i)
+        lulesh::expand_region_element(d.regionRuns.data(), (int)d.regionRuns.size(), i,
+                                      d.regNumList.data(), d.regElemlist.data(),
+                                      d.eosOrder.data());
     return copy_field(d, name, out, cap);
 }
 

@@ -139,61 +139,64 @@ static void build_corner_csr(HostDomain &d)
 }
 
 // ---- regions: CreateRegionIndexSets + sortRegions, lulesh.cu:1224-1398 ----
-static void build_regions(HostDomain &d, int nr, int balance)
+
+// The draw of CreateRegionIndexSets (lulesh.cu:1296-1351): run k covers the
+// elements from runs[k].start up to the next run's start (the last run up to
+// E) and gives them region number runs[k].region.  Only start and region
+// are filled.  A single region takes no draw.
+static std::vector<RegionRun> draw_region_runs(int rank, int E, int nr, int balance)
 {
-    GlibcRand rng((unsigned)d.rank);
-    const int myRank = d.rank;
-    const int E = d.numElem;
-    d.numReg = nr;
-    d.balance = balance;
-    d.regElemSize.assign(nr, 0);
-    d.regCSR.assign(nr, 0);
-    d.regReps.assign(nr, 0);
-    d.regSorted.assign(nr, 0);
-    d.regNumList.assign(E, 0);
-    d.regElemlist.assign(E, 0);
-    int next = 0;
+    std::vector<RegionRun> runs;
     if (nr == 1) {
-        while (next < E) d.regNumList[next++] = 1;
-    } else {
-        std::vector<int> binEnd(nr);
-        int costDen = 0;
-        for (int i = 0; i < nr; ++i) {
-            int w = 1;
-            for (int k = 0; k < balance; ++k) w *= (i + 1);
-            costDen += w;
-            binEnd[i] = costDen;
-        }
-        auto pick = [&]() {
-            int v = rng.next() % costDen, i = 0;
-            while (v >= binEnd[i]) ++i;
-            return ((i + myRank) % nr) + 1;
-        };
-        int lastReg = -1;
-        while (next < E) {
-            int regionNum = pick();
-            while (regionNum == lastReg) regionNum = pick();
-            int bin = rng.next() % 1000, elements;
-            if (bin < 773)
-                elements = rng.next() % 15 + 1;
-            else if (bin < 937)
-                elements = rng.next() % 16 + 16;
-            else if (bin < 970)
-                elements = rng.next() % 32 + 32;
-            else if (bin < 974)
-                elements = rng.next() % 64 + 64;
-            else if (bin < 978)
-                elements = rng.next() % 128 + 128;
-            else if (bin < 981)
-                elements = rng.next() % 256 + 256;
-            else
-                elements = rng.next() % 1537 + 512;
-            int runto = elements + next;
-            while (next < runto && next < E) d.regNumList[next++] = regionNum;
-            lastReg = regionNum;
-        }
+        runs.push_back({0, 1, 0, 0});
+        return runs;
     }
-    for (int i = 0; i < E; ++i) d.regElemSize[d.regNumList[i] - 1]++;
+    GlibcRand rng((unsigned)rank);
+    std::vector<int> binEnd(nr);
+    int costDen = 0;
+    for (int i = 0; i < nr; ++i) {
+        int w = 1;
+        for (int k = 0; k < balance; ++k) w *= (i + 1);
+        costDen += w;
+        binEnd[i] = costDen;
+    }
+    auto pick = [&]() {
+        int v = rng.next() % costDen, i = 0;
+        while (v >= binEnd[i]) ++i;
+        return ((i + rank) % nr) + 1;
+    };
+    int lastReg = -1, next = 0;
+    while (next < E) {
+        int regionNum = pick();
+        while (regionNum == lastReg) regionNum = pick();
+        int bin = rng.next() % 1000, elements;
+        if (bin < 773)
+            elements = rng.next() % 15 + 1;
+        else if (bin < 937)
+            elements = rng.next() % 16 + 16;
+        else if (bin < 970)
+            elements = rng.next() % 32 + 32;
+        else if (bin < 974)
+            elements = rng.next() % 64 + 64;
+        else if (bin < 978)
+            elements = rng.next() % 128 + 128;
+        else if (bin < 981)
+            elements = rng.next() % 256 + 256;
+        else
+            elements = rng.next() % 1537 + 512;
+        runs.push_back({next, regionNum, 0, 0});
+        next = std::min(next + elements, E);
+        lastReg = regionNum;
+    }
+    return runs;
+}
+
+// Rep counts per region, the stable descending bubble sort by reps that
+// carries the sizes and indices along (sortRegions), regSorted, and the
+// region starts in regCSR.  Expects d.regElemSize to hold each region's
+// element count by region index.
+static void sort_regions(HostDomain &d, int nr)
+{
     for (int r = 0; r < nr; ++r) {
         int rep;
         if (r < nr / 2)
@@ -204,7 +207,6 @@ static void build_regions(HostDomain &d, int nr, int balance)
             rep = 10 * (1 + d.cost);
         d.regReps[r] = rep;
     }
-    // stable descending bubble sort by reps carrying sizes and indices
     std::vector<int> idx(nr);
     for (int i = 0; i < nr; ++i) idx[i] = i;
     for (int i = 0; i < nr - 1; ++i)
@@ -217,6 +219,26 @@ static void build_regions(HostDomain &d, int nr, int balance)
     for (int i = 0; i < nr; ++i) d.regSorted[idx[i]] = i;
     d.regCSR[0] = 0;
     for (int i = 1; i < nr; ++i) d.regCSR[i] = d.regCSR[i - 1] + d.regElemSize[i - 1];
+}
+
+static void build_regions(HostDomain &d, int nr, int balance)
+{
+    const int E = d.numElem;
+    d.numReg = nr;
+    d.balance = balance;
+    d.regElemSize.assign(nr, 0);
+    d.regCSR.assign(nr, 0);
+    d.regReps.assign(nr, 0);
+    d.regSorted.assign(nr, 0);
+    d.regNumList.assign(E, 0);
+    d.regElemlist.assign(E, 0);
+    const std::vector<RegionRun> runs = draw_region_runs(d.rank, E, nr, balance);
+    for (size_t k = 0; k < runs.size(); ++k) {
+        const int end = k + 1 < runs.size() ? runs[k + 1].start : E;
+        for (int i = runs[k].start; i < end; ++i) d.regNumList[i] = runs[k].region;
+    }
+    for (int i = 0; i < E; ++i) d.regElemSize[d.regNumList[i] - 1]++;
+    sort_regions(d, nr);
     // fill; afterwards regCSR[r] is the END of region r, which is what the
     // EOS region lookup (giveMyRegion, lulesh.cu:3976-3984) searches
     for (int i = 0; i < E; ++i) {
@@ -249,6 +271,65 @@ static void build_regions(HostDomain &d, int nr, int balance)
         d.eosClassEnd[c] = (int)d.eosOrder.size();
         d.eosClassRep[c] = distinct[c];
     }
+}
+
+// The same region sets as build_regions, kept as runs: the per-region and
+// per-class tables are complete, regNumList, regElemlist and eosOrder stay
+// empty, and each run carries where its elements go in the last two
+// (expand_region_element writes them).  A region's runs come in ascending
+// element order, and so do a rep class's, which is the order both lists
+// hold their elements in.
+static void build_region_runs(HostDomain &d, int nr, int balance)
+{
+    const int E = d.numElem;
+    d.numReg = nr;
+    d.balance = balance;
+    d.regElemSize.assign(nr, 0);
+    d.regCSR.assign(nr, 0);
+    d.regReps.assign(nr, 0);
+    d.regSorted.assign(nr, 0);
+    d.regNumList.clear();
+    d.regElemlist.clear();
+    d.eosOrder.clear();
+    d.regionRuns = draw_region_runs(d.rank, E, nr, balance);
+    std::vector<RegionRun> &runs = d.regionRuns;
+    auto run_len = [&](size_t k) {
+        return (k + 1 < runs.size() ? runs[k + 1].start : E) - runs[k].start;
+    };
+    for (size_t k = 0; k < runs.size(); ++k) d.regElemSize[runs[k].region - 1] += run_len(k);
+    // element counts by region index, before the sort permutes them
+    const std::vector<int> count = d.regElemSize;
+    sort_regions(d, nr);
+    // rep classes: the distinct rep counts of the regions that hold
+    // elements, heaviest first, each class's elements one after the other
+    std::vector<int> distinct;
+    for (int r = 0; r < nr; ++r) {
+        if (count[r] == 0) continue;
+        const int rep = d.regReps[d.regSorted[r]];
+        if (std::find(distinct.begin(), distinct.end(), rep) == distinct.end())
+            distinct.push_back(rep);
+    }
+    std::sort(distinct.begin(), distinct.end(), [](int a, int b) { return a > b; });
+    d.eosNumClass = (int)distinct.size();
+    std::vector<int> class_at(d.eosNumClass, 0);
+    int total = 0;
+    for (int c = 0; c < d.eosNumClass; ++c) {
+        class_at[c] = total;
+        for (int r = 0; r < nr; ++r)
+            if (count[r] > 0 && d.regReps[d.regSorted[r]] == distinct[c]) total += count[r];
+        d.eosClassEnd[c] = total;
+        d.eosClassRep[c] = distinct[c];
+    }
+    for (size_t k = 0; k < runs.size(); ++k) {
+        const int r = runs[k].region - 1, s = d.regSorted[r];
+        const int c = (int)(std::find(distinct.begin(), distinct.end(), d.regReps[s]) -
+                            distinct.begin());
+        runs[k].list_at = d.regCSR[s];
+        runs[k].eos_at = class_at[c];
+        d.regCSR[s] += run_len(k);
+        class_at[c] += run_len(k);
+    }
+    // regCSR now holds each region's END, as after build_regions' fill
 }
 
 void build_domain(HostDomain &d, int nx, int tp, int col, int row, int plane,
@@ -678,7 +759,7 @@ void build_domain_light(HostDomain &d, int nx, int numReg, int balance, int cost
     double scale = nx / 45.0;
     d.einit = ebase * scale * scale * scale;
     d.deltatime = (.5 * cbrt(volo0)) / sqrt(2 * d.einit);
-    build_regions(d, numReg, balance);
+    build_region_runs(d, numReg, balance);
 }
 
 double origin_deltatime(int nx, int tp)

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "lulesh_dev.h"
+#include "region_runs.hpp"
 
 namespace lulesh {
 
@@ -49,8 +50,11 @@ struct HostDomain {
     double einit = 0.0;
     double deltatime = 0.0;  // initial dt of this domain, lulesh.cu:1205
     // geometry and connectivity left to the device (build_domain_light):
-    // the vectors from nodelist to nodalMass above are empty
+    // the vectors from nodelist to nodalMass above are empty, and so are
+    // regNumList, regElemlist and eosOrder, which the device writes from
+    // the region runs (region_runs.hpp); the other region tables are full
     bool device_geometry = false;
+    std::vector<RegionRun> regionRuns;
     // read from an lmesh file (build_domain_lmesh)
     bool unstructured = false;
     int octantCorner = 0;
@@ -73,9 +77,10 @@ void build_domain(HostDomain &d, int nx, int tp, int col, int row, int plane,
 
 // A single (tp = 1) domain with only what must come from the host: the
 // scalars, the energy deposit and initial dt, and the region sets drawn
-// from glibc rand (with the EOS order).  The geometry and connectivity are
-// generated on the device (setup.cu) with the same values build_domain
-// computes.
+// from glibc rand, as runs (regionRuns) with the per-region and per-class
+// tables.  The geometry, the connectivity and the per-element region
+// arrays are generated on the device (setup.cu) with the same values
+// build_domain computes.
 void build_domain_light(HostDomain &d, int nx, int numReg, int balance, int cost);
 
 // An unstructured domain from an lmesh file, the format the reference reads

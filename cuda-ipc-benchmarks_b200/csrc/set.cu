@@ -589,7 +589,7 @@ static bool field_of(const lulesh_set *s, int d, const char *name, FieldRef *out
         {"letap", D.letap, 4 * E}, {"lzetam", D.lzetam, 4 * E}, {"lzetap", D.lzetap, 4 * E},
         {"elemBC", D.elemBC, 4 * E}, {"matElemlist", D.matElemlist, 4 * E},
         {"regNumList", D.regNumList, 4 * E}, {"regElemlist", D.regElemlist, 4 * E},
-        {"nodeElemCount", D.nodeElemCount, 4 * N}, {"nodeElemStart", D.nodeElemStart, 4 * N},
+        {"eosOrder", D.eosOrder, 4 * E}, {"nodeElemCount", D.nodeElemCount, 4 * N}, {"nodeElemStart", D.nodeElemStart, 4 * N},
         {"nodeElemCornerList", D.nodeElemCornerList, 32 * E}, {"symmX", D.symmX, 4 * en2},
         {"symmY", D.symmY, 4 * en2}, {"symmZ", D.symmZ, 4 * en2},
         {"regCSR", D.regCSR, 4 * nr}, {"regReps", D.regReps, 4 * nr},

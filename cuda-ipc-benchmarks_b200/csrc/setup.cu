@@ -4,9 +4,11 @@
 // NewDomain (LULESH/cuda/src/lulesh.cu:750-1221) builds these arrays on the
 // host and copies them to the GPU: about 600 bytes per element.  For a
 // single domain (tp = 1) every one of them is a closed-form function of the
-// element or node position, so two kernels write them in place and only
-// the region sets (drawn from glibc rand) travel from the host.  The values
-// are those of the host builder, bit for bit:
+// element or node position, so two kernels write them in place.  The
+// region sets are drawn from glibc rand on the host, but only as runs of
+// elements (region_runs.hpp); a third kernel writes regNumList,
+// regElemlist and the EOS order from them.  The values are those of the
+// host builder, bit for bit:
 //   * this file is compiled with -fmad=false: the volume and coordinate
 //     arithmetic is not contracted into FMAs, like the reference's host code;
 //   * every expression keeps the host builder's operand order;
@@ -183,7 +185,40 @@ __global__ void k_nodal_mass(const DomDev *doms, const int2 *blocks)
     D.nodalMass[n] = m;
 }
 
+// regNumList, regElemlist and the EOS order of a single domain from its
+// region runs (CreateRegionIndexSets' fill, lulesh.cu:1343-1395): one
+// thread per element.
+__global__ void k_region_sets(const RegionRun *runs, int nruns, int E, int *regNumList,
+                              int *regElemlist, int *eosOrder)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= E) return;
+    expand_region_element(runs, nruns, i, regNumList, regElemlist, eosOrder);
+}
+
 }  // namespace
+
+int setup_regions_on_device(const DomDev &D, const std::vector<RegionRun> &runs,
+                            cudaStream_t st)
+{
+    // the runs are staged in fx_elem, which set-up zeroes and the first
+    // force pass overwrites: every run holds at least one element, so the
+    // table (16 B per run) fits in that array's 64 B per element
+    const size_t bytes = sizeof(RegionRun) * runs.size();
+    if (runs.empty() || runs.size() > (size_t)D.numElem || runs[0].start != 0) {
+        set_error("region runs do not cover the domain");
+        return LULESH_INVALID_ARG;
+    }
+    RegionRun *staged = reinterpret_cast<RegionRun *>(D.fx_elem);
+    cudaError_t e = cudaMemcpyAsync(staged, runs.data(), bytes, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return cuda_status(e, "region runs upload");
+    const int b = 128;
+    k_region_sets<<<(D.numElem + b - 1) / b, b, 0, st>>>(staged, (int)runs.size(), D.numElem,
+                                                         D.regNumList, D.regElemlist,
+                                                         D.eosOrder);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e, "region sets kernel");
+    return cuda_status(cudaMemsetAsync(staged, 0, bytes, st), "region runs clear");
+}
 
 int nodal_mass_on_device(lulesh_set *s)
 {

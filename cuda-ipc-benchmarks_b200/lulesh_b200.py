@@ -55,7 +55,7 @@ INT_FIELDS = {
     "nodelist", "lxim", "lxip", "letam", "letap", "lzetam", "lzetap", "elemBC",
     "matElemlist", "regNumList", "regElemlist", "nodeElemCount",
     "nodeElemStart", "nodeElemCornerList", "symmX", "symmY", "symmZ", "regCSR",
-    "regReps", "regSorted",
+    "regReps", "regSorted", "eosOrder",
 }
 
 # every symbol include/lulesh_b200.h declares

@@ -9,7 +9,7 @@ pytestmark = pytest.mark.gpu
 FIELDS = ["e", "p", "q", "ql", "qq", "v", "volo", "delv", "vdov", "arealg", "ss", "elemMass",
           "x", "y", "z", "xd", "yd", "zd", "nodalMass", "fx_elem", "nodelist", "lxim", "lxip",
           "letam", "letap", "lzetam", "lzetap", "elemBC", "matElemlist", "regNumList",
-          "regElemlist", "nodeElemCount", "nodeElemStart", "nodeElemCornerList", "symmX",
+          "regElemlist", "eosOrder", "nodeElemCount", "nodeElemStart", "nodeElemCornerList", "symmX",
           "symmY", "symmZ", "regCSR", "regReps", "regSorted"]
 
 
@@ -37,7 +37,8 @@ def test_batch_uses_device_setup_with_same_results(lulesh):
     with lulesh.LuleshSet.batch(jobs) as dev, \
             lulesh.LuleshSet.batch(jobs, flags=lulesh.FLAG_HOST_SETUP) as host:
         for d in range(3):
-            for name in ("x", "volo", "nodalMass", "nodeElemCornerList", "regElemlist"):
+            for name in ("x", "volo", "nodalMass", "nodeElemCornerList", "regNumList",
+                         "regElemlist", "eosOrder"):
                 assert _same(dev.field(name, d), host.field(name, d)), (d, name)
         dev.run()
         host.run()

@@ -190,3 +190,44 @@ def test_closed_form_corner_csr(host, nx):
                 got[s + r] = Ep * j + (ez * nx + ey) * nx + ex
                 r += 1
     assert np.array_equal(got, corners)
+
+
+def _light(host, name, nx, nr, b, c, dtype=np.int32):
+    n = host.lulesh_host_light_field(nx, nr, b, c, name.encode(), None, 0)
+    assert n >= 0, name
+    out = np.empty(n, dtype=dtype)
+    host.lulesh_host_light_field(nx, nr, b, c, name.encode(),
+                                 out.ctypes.data_as(ctypes.c_void_p), n)
+    return out
+
+
+@pytest.mark.parametrize("nx,nr,b,c", [(1, 11, 1, 1), (2, 5, 2, 1), (7, 11, 1, 1),
+                                       (13, 1, 1, 1), (16, 20, 4, 4), (30, 11, 1, 1),
+                                       (45, 11, 1, 1), (48, 17, 2, 2)])
+def test_region_runs_expand_to_the_host_builders_arrays(host, nx, nr, b, c):
+    """Single domains built with their geometry on the device keep the
+    region sets as runs, and the device writes regNumList, regElemlist and
+    the EOS order from them, element by element (setup.cu k_region_sets).
+    The same per-element function, run here on the host over every element,
+    gives the full host builder's arrays (pinned to the oracle above), and
+    the per-region and per-class tables built from the runs are equal too."""
+    host.lulesh_host_light_field.restype = ctypes.c_long
+    host.lulesh_host_light_field.argtypes = [ctypes.c_int] * 4 + [ctypes.c_char_p,
+                                                                 ctypes.c_void_p, ctypes.c_long]
+    E = nx ** 3
+    for f in ("regNumList", "regElemlist", "eosOrder", "regElemSize", "regCSR", "regReps",
+              "regSorted", "eosClassEnd", "eosClassRep"):
+        got = _light(host, f, nx, nr, b, c)
+        n = host.lulesh_host_domain_field(nx, 1, 0, 0, 0, 0, nr, b, c, 0, f.encode(), None, 0)
+        want = np.empty(n, dtype=np.int32)
+        host.lulesh_host_domain_field(nx, 1, 0, 0, 0, 0, nr, b, c, 0, f.encode(),
+                                      want.ctypes.data_as(ctypes.c_void_p), n)
+        assert got.size > 0 and np.array_equal(got, want), f
+    # every element written once in each list (the expansion starts from -1)
+    for f in ("regElemlist", "eosOrder"):
+        assert np.array_equal(np.sort(_light(host, f, nx, nr, b, c)), np.arange(E)), f
+    # about one run per 38 elements is what travels to the device
+    nruns = _light(host, "nruns", nx, nr, b, c, dtype=np.int64)[0]
+    assert 1 <= nruns <= E
+    if nr > 1 and E >= 20000:
+        assert nruns < E / 20
