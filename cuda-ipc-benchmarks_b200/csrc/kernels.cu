@@ -659,7 +659,17 @@ __device__ __forceinline__ void calc_pressure(double &p_new, double &bvc, double
     p_new = p_temp;
 }
 
+// x / rho0 (the reference density).  With RHO1 the density is 1.0, and
+// x / 1.0 is x exactly in IEEE-754 arithmetic, so the division is left
+// out; the results are the same bits either way.
+template <bool RHO1>
+__device__ __forceinline__ double per_rho0(double x, double rho0)
+{
+    return RHO1 ? x : x / rho0;
+}
+
 // CalcEnergyForElems_device, lulesh.cu:3867-3974
+template <bool RHO1>
 __device__ __forceinline__ void calc_energy(double &p_new, double &e_new, double &q_new,
                                             double &bvc, double &pbvc, double &p_old,
                                             double &e_old, double &q_old, double &compression,
@@ -678,7 +688,7 @@ __device__ __forceinline__ void calc_energy(double &p_new, double &e_new, double
     if (delvc > 0.) {
         q_new = 0.;
     } else {
-        double ssc = (pbvc * e_new + vhalf * vhalf * bvc * pHalfStep) / rho0;
+        double ssc = per_rho0<RHO1>(pbvc * e_new + vhalf * vhalf * bvc * pHalfStep, rho0);
         if (ssc <= .1111111e-36)
             ssc = .3333333e-18;
         else
@@ -694,7 +704,7 @@ __device__ __forceinline__ void calc_energy(double &p_new, double &e_new, double
     if (delvc > 0.) {
         q_tilde = 0.;
     } else {
-        double ssc = (pbvc * e_new + vnewc * vnewc * bvc * p_new) / rho0;
+        double ssc = per_rho0<RHO1>(pbvc * e_new + vnewc * vnewc * bvc * p_new, rho0);
         if (ssc <= .1111111e-36)
             ssc = .3333333e-18;
         else
@@ -707,13 +717,53 @@ __device__ __forceinline__ void calc_energy(double &p_new, double &e_new, double
     if (e_new < emin) e_new = emin;
     calc_pressure(p_new, bvc, pbvc, e_new, compression, vnewc, pmin, p_cut, eosvmax);
     if (delvc <= 0.) {
-        double ssc = (pbvc * e_new + vnewc * vnewc * bvc * p_new) / rho0;
+        double ssc = per_rho0<RHO1>(pbvc * e_new + vnewc * vnewc * bvc * p_new, rho0);
         if (ssc <= .1111111e-36)
             ssc = .3333333e-18;
         else
             ssc = sqrt(ssc);
         q_new = (ssc * ql + qq);
         if (fabs(q_new) < q_cut) q_new = 0.;
+    }
+}
+
+// The rep loop of ApplyMaterialPropertiesAndUpdateVolume_kernel
+// (lulesh.cu:4045-4083), the reference's cost model: every rep re-evaluates
+// the EOS from the same inputs (the loop is pure).
+template <bool RHO1>
+__device__ __forceinline__ void eos_reps(int rep, double e_temp, double p_temp, double q_temp,
+                                         double qq_temp, double ql_temp, double delvc_temp,
+                                         double vnewc, double eosvmin, double eosvmax,
+                                         double rho0, const Params &P, double &p_new,
+                                         double &e_new, double &q_new, double &bvc,
+                                         double &pbvc)
+{
+    double e_old, delvc, p_old, q_old, compression, compHalfStep, qq_old, ql_old, work;
+    for (int r = 0; r < rep; r++) {
+        e_old = e_temp;
+        p_old = p_temp;
+        q_old = q_temp;
+        qq_old = qq_temp;
+        ql_old = ql_temp;
+        delvc = delvc_temp;
+        work = 0.;
+        double vchalf;
+        compression = 1. / vnewc - 1.;
+        vchalf = vnewc - delvc * .5;
+        compHalfStep = 1. / vchalf - 1.;
+        if (eosvmin != 0.) {
+            if (vnewc <= eosvmin) compHalfStep = compression;
+        }
+        if (eosvmax != 0.) {
+            if (vnewc >= eosvmax) {
+                p_old = 0.;
+                compression = 0.;
+                compHalfStep = 0.;
+            }
+        }
+        calc_energy<RHO1>(p_new, e_new, q_new, bvc, pbvc, p_old, e_old, q_old, compression,
+                          compHalfStep, vnewc, work, delvc, P.pmin, P.p_cut, P.e_cut, P.q_cut,
+                          P.emin, qq_old, ql_old, rho0, eosvmax);
     }
 }
 
@@ -725,8 +775,9 @@ __device__ __forceinline__ double warp_min(double v)
 }
 
 // SUB: a subdomain set's fused cycle, which reads a comm face's neighbour
-// element in the neighbouring subdomain (no MonoQ ghost copy)
-template <int BS, bool U = false, bool SUB = false>
+// element in the neighbouring subdomain (no MonoQ ghost copy).
+// RHO1: the reference density P.refdens is 1.0 (per_rho0).
+template <int BS, bool U = false, bool SUB = false, bool RHO1 = false>
 __global__ void __launch_bounds__(BS, min_blocks(kEosMinBlocks, BS)) k_eos(SetArgs a, Params P)
 {
     pdl_enter();
@@ -862,49 +913,19 @@ __global__ void __launch_bounds__(BS, min_blocks(kEosMinBlocks, BS)) k_eos(SetAr
         }
         if (vc <= 0.) atomicMin(&T.bad_vol, zidx);
 
-        double e_old, delvc, p_old, q_old, compression, compHalfStep, qq_old, ql_old, work;
         double p_new = 0., e_new = 0., q_new = 0., bvc = 0., pbvc = 0.;
         const double e_temp = D.e[zidx];
         const double p_temp = D.p[zidx];
-        const double q_temp = q_old_z;
-        const double qq_temp = qquad;
-        const double ql_temp = qlin;
         const double delvc_temp = D.delv[zidx];
-        double rho0 = P.refdens;
-        // The reference's cost model: every rep re-evaluates the EOS from
-        // the same inputs (the loop is pure), lulesh.cu:4045-4083.
-        for (int r = 0; r < rep; r++) {
-            e_old = e_temp;
-            p_old = p_temp;
-            q_old = q_temp;
-            qq_old = qq_temp;
-            ql_old = ql_temp;
-            delvc = delvc_temp;
-            work = 0.;
-            double vchalf;
-            compression = 1. / vnewc - 1.;
-            vchalf = vnewc - delvc * .5;
-            compHalfStep = 1. / vchalf - 1.;
-            if (eosvmin != 0.) {
-                if (vnewc <= eosvmin) compHalfStep = compression;
-            }
-            if (eosvmax != 0.) {
-                if (vnewc >= eosvmax) {
-                    p_old = 0.;
-                    compression = 0.;
-                    compHalfStep = 0.;
-                }
-            }
-            calc_energy(p_new, e_new, q_new, bvc, pbvc, p_old, e_old, q_old, compression,
-                        compHalfStep, vnewc, work, delvc, P.pmin, P.p_cut, P.e_cut, P.q_cut,
-                        P.emin, qq_old, ql_old, rho0, eosvmax);
-        }
+        const double rho0 = P.refdens;
+        eos_reps<RHO1>(rep, e_temp, p_temp, q_old_z, qquad, qlin, delvc_temp, vnewc, eosvmin,
+                       eosvmax, rho0, P, p_new, e_new, q_new, bvc, pbvc);
         D.p[zidx] = p_new;
         D.e[zidx] = e_new;
         D.q[zidx] = q_new;
 
         // CalcSoundSpeedForElems_device, lulesh.cu:3795-3809
-        double ssTmp = (pbvc * e_new + vnewc * vnewc * bvc * p_new) / rho0;
+        double ssTmp = per_rho0<RHO1>(pbvc * e_new + vnewc * vnewc * bvc * p_new, rho0);
         if (ssTmp <= .1111111e-36)
             ssTmp = .3333333e-18;
         else
@@ -952,22 +973,38 @@ __global__ void __launch_bounds__(BS, min_blocks(kEosMinBlocks, BS)) k_eos(SetAr
     }
 }
 
-void launch_eos(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs, bool u,
-                bool sub)
+template <bool RHO1>
+static void launch_eos_variant(const SetArgs &a, int nblocks, const Params &P, cudaStream_t s,
+                               int bs, bool u, bool sub)
 {
     if (u) {
-        launch_k(k_eos<kElemBlock, true>, nblocks, kElemBlock, s, a.pdl != 0, a, P);
+        launch_k(k_eos<kElemBlock, true, false, RHO1>, nblocks, kElemBlock, s, a.pdl != 0, a, P);
         return;
     }
     if (sub) {  // subdomain sets take 128-element blocks only
-        launch_k(k_eos<kElemBlock, false, true>, nblocks, kElemBlock, s, a.pdl != 0, a, P);
+        launch_k(k_eos<kElemBlock, false, true, RHO1>, nblocks, kElemBlock, s, a.pdl != 0, a,
+                 P);
         return;
     }
     switch (bs) {
-        case 64: launch_k(k_eos<64>, nblocks, 64, s, a.pdl != 0, a, P); break;
-        case 256: launch_k(k_eos<256>, nblocks, 256, s, a.pdl != 0, a, P); break;
-        default: launch_k(k_eos<kElemBlock>, nblocks, kElemBlock, s, a.pdl != 0, a, P); break;
+        case 64: launch_k(k_eos<64, false, false, RHO1>, nblocks, 64, s, a.pdl != 0, a, P); break;
+        case 256:
+            launch_k(k_eos<256, false, false, RHO1>, nblocks, 256, s, a.pdl != 0, a, P);
+            break;
+        default:
+            launch_k(k_eos<kElemBlock, false, false, RHO1>, nblocks, kElemBlock, s, a.pdl != 0,
+                     a, P);
+            break;
     }
+}
+
+void launch_eos(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs, bool u,
+                bool sub)
+{
+    if (P.refdens == 1.0)  // every sedov problem (default_params)
+        launch_eos_variant<true>(a, nblocks, P, s, bs, u, sub);
+    else
+        launch_eos_variant<false>(a, nblocks, P, s, bs, u, sub);
 }
 
 // ---------------------------------------------------------------------------
