@@ -775,9 +775,8 @@ __device__ __forceinline__ double warp_min(double v)
 }
 
 // SUB: a subdomain set's fused cycle, which reads a comm face's neighbour
-// element in the neighbouring subdomain (no MonoQ ghost copy).
-// RHO1: the reference density P.refdens is 1.0 (per_rho0).
-template <int BS, bool U = false, bool SUB = false, bool RHO1 = false>
+// element in the neighbouring subdomain (no MonoQ ghost copy)
+template <int BS, bool U = false, bool SUB = false>
 __global__ void __launch_bounds__(BS, min_blocks(kEosMinBlocks, BS)) k_eos(SetArgs a, Params P)
 {
     pdl_enter();
@@ -918,14 +917,21 @@ __global__ void __launch_bounds__(BS, min_blocks(kEosMinBlocks, BS)) k_eos(SetAr
         const double p_temp = D.p[zidx];
         const double delvc_temp = D.delv[zidx];
         const double rho0 = P.refdens;
-        eos_reps<RHO1>(rep, e_temp, p_temp, q_old_z, qquad, qlin, delvc_temp, vnewc, eosvmin,
-                       eosvmax, rho0, P, p_new, e_new, q_new, bvc, pbvc);
+        // the reference density is 1.0 in every sedov problem (uniform branch)
+        const bool rho1 = rho0 == 1.0;
+        if (rho1)
+            eos_reps<true>(rep, e_temp, p_temp, q_old_z, qquad, qlin, delvc_temp, vnewc,
+                           eosvmin, eosvmax, rho0, P, p_new, e_new, q_new, bvc, pbvc);
+        else
+            eos_reps<false>(rep, e_temp, p_temp, q_old_z, qquad, qlin, delvc_temp, vnewc,
+                            eosvmin, eosvmax, rho0, P, p_new, e_new, q_new, bvc, pbvc);
         D.p[zidx] = p_new;
         D.e[zidx] = e_new;
         D.q[zidx] = q_new;
 
         // CalcSoundSpeedForElems_device, lulesh.cu:3795-3809
-        double ssTmp = per_rho0<RHO1>(pbvc * e_new + vnewc * vnewc * bvc * p_new, rho0);
+        double ssTmp = pbvc * e_new + vnewc * vnewc * bvc * p_new;
+        if (!rho1) ssTmp = ssTmp / rho0;
         if (ssTmp <= .1111111e-36)
             ssTmp = .3333333e-18;
         else
@@ -973,38 +979,22 @@ __global__ void __launch_bounds__(BS, min_blocks(kEosMinBlocks, BS)) k_eos(SetAr
     }
 }
 
-template <bool RHO1>
-static void launch_eos_variant(const SetArgs &a, int nblocks, const Params &P, cudaStream_t s,
-                               int bs, bool u, bool sub)
-{
-    if (u) {
-        launch_k(k_eos<kElemBlock, true, false, RHO1>, nblocks, kElemBlock, s, a.pdl != 0, a, P);
-        return;
-    }
-    if (sub) {  // subdomain sets take 128-element blocks only
-        launch_k(k_eos<kElemBlock, false, true, RHO1>, nblocks, kElemBlock, s, a.pdl != 0, a,
-                 P);
-        return;
-    }
-    switch (bs) {
-        case 64: launch_k(k_eos<64, false, false, RHO1>, nblocks, 64, s, a.pdl != 0, a, P); break;
-        case 256:
-            launch_k(k_eos<256, false, false, RHO1>, nblocks, 256, s, a.pdl != 0, a, P);
-            break;
-        default:
-            launch_k(k_eos<kElemBlock, false, false, RHO1>, nblocks, kElemBlock, s, a.pdl != 0,
-                     a, P);
-            break;
-    }
-}
-
 void launch_eos(const SetArgs &a, int nblocks, Params P, cudaStream_t s, int bs, bool u,
                 bool sub)
 {
-    if (P.refdens == 1.0)  // every sedov problem (default_params)
-        launch_eos_variant<true>(a, nblocks, P, s, bs, u, sub);
-    else
-        launch_eos_variant<false>(a, nblocks, P, s, bs, u, sub);
+    if (u) {
+        launch_k(k_eos<kElemBlock, true>, nblocks, kElemBlock, s, a.pdl != 0, a, P);
+        return;
+    }
+    if (sub) {  // subdomain sets take 128-element blocks only
+        launch_k(k_eos<kElemBlock, false, true>, nblocks, kElemBlock, s, a.pdl != 0, a, P);
+        return;
+    }
+    switch (bs) {
+        case 64: launch_k(k_eos<64>, nblocks, 64, s, a.pdl != 0, a, P); break;
+        case 256: launch_k(k_eos<256>, nblocks, 256, s, a.pdl != 0, a, P); break;
+        default: launch_k(k_eos<kElemBlock>, nblocks, kElemBlock, s, a.pdl != 0, a, P); break;
+    }
 }
 
 // ---------------------------------------------------------------------------
