@@ -88,8 +88,9 @@ BUILD_BYTES_STEP = bytes_model.step_bytes(bytes_model.THIS_BUILD)
 LAUNCHES_PER_CYCLE = 5  # time_increment, force, nodal, kinematics, eos
 # FP64 flops per element of each phase (an FMA counts 2), measured with
 # ncu's smsp__sass_thread_inst_executed_op_{dfma,dadd,dmul}_pred_on counters
-# at -s 64 (profiles/cycle_kernels_s64_full.md); nodal is per node.
-FP64_FLOPS = {"force": 1427.0, "nodal": 50.2, "kinematics": 814.0, "eos": 510.4}
+# at -s 64 (profiles/cycle_kernels_s64_full.md; the EOS after its
+# unit-density form, profiles/eos_unit_density_s64.md); nodal is per node.
+FP64_FLOPS = {"force": 1427.0, "nodal": 50.2, "kinematics": 814.0, "eos": 359.9}
 
 
 def fp64_peak_tflops(dev):
