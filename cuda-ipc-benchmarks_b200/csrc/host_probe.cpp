@@ -3,6 +3,7 @@
 // arithmetic and index layout against the oracle without a GPU.  Not part
 // of the drop-in ABI (include/lulesh_b200.h).
 #include <cstring>
+#include <vector>
 
 #include "host_setup.hpp"
 
@@ -94,6 +95,11 @@ long lulesh_host_light_field(int nx, int numReg, int balance, int cost, const ch
         if (out && cap >= 1) *(long *)out = (long)d.regionRuns.size();
         return 1;
     }
+    if (!std::strcmp(name, "runs")) {  // start, region, list_at, eos_at per run
+        const long n = 4 * (long)d.regionRuns.size();
+        if (out && cap >= n) std::memcpy(out, d.regionRuns.data(), sizeof(int) * n);
+        return n;
+    }
     const int E = d.numElem;
     d.regNumList.assign(E, -1);
     d.regElemlist.assign(E, -1);
@@ -103,6 +109,16 @@ long lulesh_host_light_field(int nx, int numReg, int balance, int cost, const ch
                                       d.regNumList.data(), d.regElemlist.data(),
                                       d.eosOrder.data());
     return copy_field(d, name, out, cap);
+}
+
+// region_runs_valid on a caller's table of nruns runs, four ints each
+// (start, region, list_at, eos_at), over E elements: 1 valid, 0 not.
+int lulesh_host_region_runs_valid(const int *runs4, int nruns, int E)
+{
+    std::vector<lulesh::RegionRun> runs(nruns > 0 ? nruns : 0);
+    for (int k = 0; k < nruns; ++k)
+        runs[k] = {runs4[4 * k], runs4[4 * k + 1], runs4[4 * k + 2], runs4[4 * k + 3]};
+    return lulesh::region_runs_valid(runs.data(), nruns, E) ? 1 : 0;
 }
 
 // Read one domain from an lmesh file (lulesh_create_from_mesh's reader) and

@@ -52,4 +52,22 @@ LULESH_HD inline void expand_region_element(const RegionRun *runs, int nruns, in
     eosOrder[r.eos_at + k] = i;
 }
 
+// True when runs[0..nruns) cover [0, E) as expand_region_element expects
+// and every write it makes stays inside the three E-element arrays: starts
+// strictly increasing from 0, at most E runs, and each run's elements
+// fitting in regElemlist and the EOS order from its two positions.  Checked
+// on the host before the runs go to the device.
+inline bool region_runs_valid(const RegionRun *runs, int nruns, int E)
+{
+    if (!runs || nruns < 1 || nruns > E || runs[0].start != 0) return false;
+    for (int k = 0; k < nruns; ++k) {
+        const int end = k + 1 < nruns ? runs[k + 1].start : E;
+        if (end <= runs[k].start || end > E) return false;
+        const int len = end - runs[k].start;
+        if (runs[k].list_at < 0 || runs[k].list_at > E - len) return false;
+        if (runs[k].eos_at < 0 || runs[k].eos_at > E - len) return false;
+    }
+    return true;
+}
+
 }  // namespace lulesh

@@ -205,7 +205,8 @@ int setup_regions_on_device(const DomDev &D, const std::vector<RegionRun> &runs,
     // force pass overwrites: every run holds at least one element, so the
     // table (16 B per run) fits in that array's 64 B per element
     const size_t bytes = sizeof(RegionRun) * runs.size();
-    if (runs.empty() || runs.size() > (size_t)D.numElem || runs[0].start != 0) {
+    if (runs.size() > (size_t)D.numElem ||
+        !region_runs_valid(runs.data(), (int)runs.size(), D.numElem)) {
         set_error("region runs do not cover the domain");
         return LULESH_INVALID_ARG;
     }

@@ -231,3 +231,38 @@ def test_region_runs_expand_to_the_host_builders_arrays(host, nx, nr, b, c):
     assert 1 <= nruns <= E
     if nr > 1 and E >= 20000:
         assert nruns < E / 20
+
+
+def test_region_runs_are_checked_before_they_reach_the_device(host):
+    """setup_regions_on_device refuses a run table whose expansion would
+    write outside the three per-element arrays (region_runs_valid); the
+    tables the light builder draws pass, tampered ones do not."""
+    host.lulesh_host_light_field.restype = ctypes.c_long
+    host.lulesh_host_light_field.argtypes = [ctypes.c_int] * 4 + [ctypes.c_char_p,
+                                                                 ctypes.c_void_p, ctypes.c_long]
+    host.lulesh_host_region_runs_valid.restype = ctypes.c_int
+    host.lulesh_host_region_runs_valid.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+
+    def valid(t, E):
+        t = np.ascontiguousarray(t, dtype=np.int32)
+        return host.lulesh_host_region_runs_valid(t.ctypes.data_as(ctypes.c_void_p),
+                                                  t.shape[0], E) == 1
+
+    for nx, nr in [(1, 11), (2, 1), (9, 5), (20, 11), (33, 20)]:
+        t = _light(host, "runs", nx, nr, 1, 1).reshape(-1, 4)
+        E = nx ** 3
+        assert valid(t, E), (nx, nr)
+        if t.shape[0] < 2:
+            continue
+        bad = t.copy(); bad[0, 0] = 1                      # does not start at element 0
+        assert not valid(bad, E)
+        bad = t.copy(); bad[1, 0] = bad[0, 0]              # empty run
+        assert not valid(bad, E)
+        bad = t.copy(); bad[-1, 0] = E                     # a run past the last element
+        assert not valid(bad, E)
+        bad = t.copy(); bad[-1, 2] = E                     # regElemlist write past the end
+        assert not valid(bad, E)
+        bad = t.copy(); bad[0, 3] = -1                     # EOS-order write before the start
+        assert not valid(bad, E)
+        assert not valid(t, t.shape[0] - 1)                # more runs than elements
+    assert not valid(np.zeros((0, 4)), 8)                  # no runs at all
