@@ -88,3 +88,19 @@ def test_oracle_matches_reference_cuda_build(oracle_mod, key):
     st, n = o.run(gold["its"])
     assert st == 0 and n == gold["cycles"]
     assert rel(o.origin_energy(), gold["energy"]) < 1e-12
+
+
+def test_oracle_full_run_matches_reference_cuda_build(oracle_mod):
+    """The whole -s 30 problem, run to the stop time as the reference's
+    default does (its = -1 in tests/golden/cuda_reference.json): the oracle
+    stops at the reference CUDA build's cycle (932), with its energy to
+    1e-12 and a plane-0 symmetry as small as the reference's.  About 30 s
+    on one core: this pins the oracle's time control (dt constraints,
+    TimeIncrement's clamps and the final stop) over a complete run."""
+    gold = _cuda_gold()["-s 30 -i -1"]
+    o = oracle_mod.Oracle(gold["nx"])
+    st, n = o.run(9999999)
+    assert st == 0 and n == gold["cycles"] == 932
+    assert rel(o.origin_energy(), gold["energy"]) < 1e-12
+    ma, ta, mr = o.symmetry()
+    assert mr < 1e-10 and gold["max_rel"] < 1e-10
