@@ -1,8 +1,8 @@
 // server.cu -- continuous batching of sedov jobs on one GPU.
 //
-// Submitted jobs get their region sets (glibc rand) on host worker threads
-// (build_domain_light); their geometry is generated on the device at
-// admission (setup.cu).  lulesh_server_step then
+// Submitted jobs draw their region runs (glibc rand) on host worker threads
+// (build_domain_light); their geometry and per-element region arrays are
+// generated on the device at admission (setup.cu).  lulesh_server_step then
 //   1. waits for the previous step, reads every slot's time control and
 //      origin energy (one gather kernel + two small copies issued at the end
 //      of that step) and retires finished jobs, freeing their memory;
